@@ -1,0 +1,133 @@
+"""ctypes binding of libcfdgpu.so (include/cfdgpu.h).
+
+The library is the only compute path: if it is missing or cannot be loaded,
+every entry point raises. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libcfdgpu.so"
+
+CFD_OK = 0
+ERRORS = {
+    -1: "CFD_ERR_CONFIG",
+    -2: "CFD_ERR_CUDA",
+    -3: "CFD_ERR_NONFINITE",
+    -4: "CFD_ERR_NEGATIVE_STATE",
+    -5: "CFD_ERR_TIMEOUT",
+    -6: "CFD_ERR_UNSUPPORTED",
+    -7: "CFD_ERR_NOMEM",
+}
+
+
+class CfdError(RuntimeError):
+    def __init__(self, code: int, msg: str = ""):
+        self.code = code
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+
+
+class CfdConfig(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int),
+        ("n", C.c_int * 3),
+        ("h", C.c_double * 3),
+        ("x0", C.c_double * 3),
+        ("n_ghost", C.c_int),
+        ("gamma", C.c_double),
+        ("inter_method", C.c_int),
+        ("flux_method", C.c_int),
+        ("diff_method", C.c_int),
+        ("precision", C.c_int),
+        ("strict", C.c_int),
+        ("bc", (C.c_int * 2) * 3),
+        ("device", C.c_int),
+        ("seg_len", C.c_int * 3),
+    ]
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "cfd_config_default": (None, [C.POINTER(CfdConfig)]),
+    "cfd_create": (C.c_int, [C.POINTER(CfdConfig), C.POINTER(C.c_void_p)]),
+    "cfd_destroy": (None, [C.c_void_p]),
+    "cfd_last_error": (C.c_char_p, [C.c_void_p]),
+    "cfd_set_line_bc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_int,
+                                  C.c_void_p]),
+    "cfd_upload_cons": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_download_cons": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_download_prim": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "cfd_max_dt": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
+    "cfd_rk3_step": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "cfd_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
+                          C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
+    "cfd_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong),
+                                   C.POINTER(C.c_void_p)]),
+    "cfd_set_state_device": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "cfd_version": (C.c_char_p, []),
+}
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load libcfdgpu.so (raises if it is absent: there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m cfd_inwsl_b200.build_ext`")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_PROTOS)
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != CFD_OK:
+        msg = ""
+        if handle is not None:
+            m = load().cfd_last_error(handle)
+            msg = m.decode() if m else ""
+        raise CfdError(rc, msg)
+
+
+def ptr(a: np.ndarray) -> C.c_void_p:
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+def eval_inter5(inter_method: int, q: np.ndarray, strict: bool = True) -> np.ndarray:
+    """Device interpolator on rows of q (n x 5)."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    n = q.shape[0]
+    out = np.empty(n)
+    check(load().cfd_eval_inter5(inter_method, int(strict), ptr(q), n, ptr(out)))
+    return out
+
+
+def eval_flux(dim: int, ax: int, flux_method: int, lr: np.ndarray, strict: bool = True) -> np.ndarray:
+    """Device Riemann flux on rows of lr (n x 2*nvar: left prim | right prim)."""
+    lr = np.ascontiguousarray(lr, dtype=np.float64)
+    nv = dim + 2
+    n = lr.shape[0]
+    out = np.empty((n, nv))
+    check(load().cfd_eval_flux(dim, ax, flux_method, int(strict), ptr(lr), n, ptr(out)))
+    return out

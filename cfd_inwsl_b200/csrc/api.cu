@@ -1,0 +1,727 @@
+// C ABI of the zone_FD RHS + SSP-RK3 library (include/cfdgpu.h).
+//
+// Host orchestration of the sweep kernels: boundary wiring tables, state
+// buffers, stage sequencing of BlockSolver::RK3_SSP (blockSolver.cpp:43-87),
+// the CFL step of getTimeIntervalExplicit (blockSolver.cpp:318-349) and the
+// device-resident loop of stepsLoopCFL (blockSolver.cpp:170-235).
+//
+// This translation unit is compiled with --fmad=false: its small kernels
+// (layout transposes, wave-speed reduction, step control) reproduce the
+// reference's arithmetic bit for bit.
+#include "cfdgpu.h"
+#include "euler_math.cuh"
+#include "sweep_dispatch.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using cfd::BcLine;
+using cfd::SweepParams;
+
+namespace {
+
+constexpr int kGhost = 4;
+
+// ------------------------------------------------------------------ kernels
+
+template <int NV>
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__restrict__ soa, long long ncell)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) soa[v * ncell + c] = aos[c * NV + v];
+    }
+}
+
+template <int NV>
+__global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__restrict__ aos, long long ncell, int to_prim)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        double x[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) x[v] = soa[v * ncell + c];
+        if (to_prim) {
+            double p[NV];
+            cfd::cons_to_prim<NV>(x, p);
+#pragma unroll
+            for (int v = 0; v < NV; v++) x[v] = p[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) aos[c * NV + v] = x[v];
+    }
+}
+
+// Per-direction max of (sqrt(gamma p / rho) + |u_d|) / h_d over the state,
+// as getTimeIntervalExplicit's OpenMP max loops (blockSolver.cpp:327-338).
+template <int NV>
+__global__ void __launch_bounds__(256) wave_speed_kernel(const double *__restrict__ u, long long ncell, double h0,
+                                                          double h1, double h2, unsigned long long *red)
+{
+    double lam[3] = {0.0, 0.0, 0.0};
+    const double hd[3] = {h0, h1, h2};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        double x[NV], p[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) x[v] = u[v * ncell + c];
+        cfd::cons_to_prim<NV>(x, p);
+        double cs = sqrt(cfd::kGamma * p[NV - 1] / p[0]);
+#pragma unroll
+        for (int d = 0; d < NV - 2; d++) lam[d] = fmax(lam[d], (cs + fabs(p[1 + d])) / hd[d]);
+    }
+    cfd::block_max_reduce<256, 4>(0.0, lam, red);
+}
+
+// Pointwise test kernels.
+template <int FAM>
+__global__ void eval_inter5_kernel(const double *q, int n, double c, double *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = cfd::inter5<FAM>(q[5 * i], q[5 * i + 1], q[5 * i + 2], q[5 * i + 3], q[5 * i + 4], c);
+}
+
+template <int NV, int AX, int FLUX>
+__global__ void eval_flux_kernel(const double *lr, int n, double *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        double L[NV], R[NV], f[NV];
+        for (int v = 0; v < NV; v++) {
+            L[v] = lr[2 * NV * i + v];
+            R[v] = lr[2 * NV * i + NV + v];
+        }
+        cfd::riemann<NV, AX, FLUX>(L, R, f);
+        for (int v = 0; v < NV; v++) out[NV * i + v] = f[v];
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+
+struct InterMap {
+    int fam;
+    double c;
+    bool ok;
+};
+
+// InterMethod (macro.hpp:37-78) -> interpolator family, following the
+// Euler branches of SolverType::initReconer (solverType.cpp:217-598).
+InterMap map_inter_method(int m, int dim)
+{
+    switch (m) {
+    case 2: return {cfd::FAM_WCNS5, 0.0, true};                 // WCNS5 -> weno5_JSchen
+    case 3: return {cfd::FAM_WENOZ, 0.0, true};                 // WCNSZ5 -> weno5_Z
+    case 11: return {cfd::FAM_TENOZ, 1e-5, true};               // TCNS5 -> Teno5_Z
+    case 12: return {cfd::FAM_TENOZ, 1e-4, true};               // TCNS5CT4 -> Teno5_ZCT4
+    case 13: return {cfd::FAM_TENOZ, 1e-7, true};               // TCNS5CT7 -> Teno5_ZCT7
+    case 22: return {cfd::FAM_TENOZ, 1e-5, true};               // congTCNS5CT5 -> congTcns5_ZCT5
+    case 23: return {cfd::FAM_TENOZ, 1e-10, true};              // congTCNS5CT10 -> congTcns5_ZCT10
+    case 35: return {cfd::FAM_TENOZ, 1e-5, true};               // new_TCNS5 -> new_Teno5_Z
+    case 8: return {cfd::FAM_TENOCONG, 0.15704178024750198, true};   // WCNS5CONGZ -> Teno5_CongZ
+    case 37: return {cfd::FAM_TENOCONG, 0.15704178024750198, true};  // new_WCNS5CONGZ -> new_Teno5_CongZ
+    case 9: return {cfd::FAM_TENOCONG, 0.23050581003334941, true};   // WCNS5CONGZCT4 -> Teno5_CongZCT4
+    case 10:
+        // WCNS5CONGZCT7: Teno5_CongZCT7 in 2D, but Teno5_CongAA in 1D (solverType.cpp:248-250).
+        if (dim == 1) return {0, 0.0, false};
+        return {cfd::FAM_TENOCONG, 0.072892337360747711, true};
+    case 15: return {cfd::FAM_MUSCL, 0.0, true};                // MUCSLIN5 -> musclIn5
+    case 0: case 1: case 4: case 5: case 6: case 7: case 14: case 16:
+        return {cfd::FAM_WCNS5, 0.0, true};                     // selector default: weno5_JSchen
+    default:
+        return {0, 0.0, false};                                 // TENO-A/AS research variants
+    }
+}
+
+} // namespace
+
+struct cfd_handle {
+    cfd_config cfg;
+    int dim = 0, nv = 0;
+    long long ncell = 0;
+    long long stride[3] = {1, 1, 1};
+    int fam = 0;
+    double icst = 0.0;
+    bool strict = false;
+    cudaStream_t stream = nullptr;
+    double *u[3] = {nullptr, nullptr, nullptr};
+    int cur = 0;
+    double *rhs = nullptr;
+    double *stage = nullptr;  // AoS staging buffer
+    unsigned long long *red = nullptr;
+    unsigned *err = nullptr;
+    std::vector<BcLine> bc_lo[3], bc_hi[3];
+    std::vector<double> bc_vals;
+    BcLine *d_bclo[3] = {nullptr, nullptr, nullptr};
+    BcLine *d_bchi[3] = {nullptr, nullptr, nullptr};
+    double *d_bcvals = nullptr;
+    size_t d_bcvals_cap = 0;
+    bool bc_dirty = true;
+    int seg_len[3] = {1, 1, 1};
+    bool ws_valid = false;       // red[1..3] hold the wave speeds of the current state
+    double dm_u = 0.0, dm_v = 0.0;
+    std::string msg;
+};
+
+namespace {
+
+int fail(cfd_handle *h, int code, const std::string &m)
+{
+    if (h) h->msg = m;
+    return code;
+}
+
+int cuda_fail(cfd_handle *h, cudaError_t e, const char *what)
+{
+    return fail(h, CFD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CFD_CUDA(h, call)                                  \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+long long nlines(const cfd_handle *h, int d) { return h->ncell / h->cfg.n[d]; }
+
+void transverse_axes(int d, int &t0, int &t1)
+{
+    t0 = (d == 0) ? 1 : 0;
+    t1 = (d == 2) ? 1 : 2;
+}
+
+// Cell-centre coordinate as Initializer::initUniformBlock computes it
+// (initializer.cpp:676-677): every direction starts from calZone[0].
+double cell_coor(const cfd_handle *h, long long cell, int idim)
+{
+    long long idx[3];
+    idx[0] = cell % h->cfg.n[0];
+    idx[1] = (cell / h->cfg.n[0]) % h->cfg.n[1];
+    idx[2] = cell / ((long long)h->cfg.n[0] * h->cfg.n[1]);
+    return h->cfg.x0[0] + (idx[idim] + 0.5) * h->cfg.h[0];
+}
+
+void set_line(cfd_handle *h, int d, long long lid, int side, int type, long long i0, int offset, int slot)
+{
+    BcLine b;
+    std::memset(&b, 0, sizeof(b));
+    b.slot = slot;
+    if (type == CFD_BND_PERIODIC_WRAP) {
+        // true wrap: the low end copies the far end of the line and vice versa
+        int t0, t1;
+        transverse_axes(d, t0, t1);
+        long long a = lid % h->cfg.n[t0], bb = lid / h->cfg.n[t0];
+        long long base = a * h->stride[t0] + bb * h->stride[t1];
+        long long last = base + (long long)(h->cfg.n[d] - 1) * h->stride[d];
+        b.type = cfd::BND_PERIODIC1D;
+        b.i0 = side == 0 ? last : base;
+        b.offset = side == 0 ? -(int)h->stride[d] : (int)h->stride[d];
+    } else {
+        b.type = type;
+        b.i0 = i0;
+        b.offset = offset;
+    }
+    if (b.type == cfd::BND_DOUBLEMACHUP) {
+        // OneDBnd::setCoor as wired by initDoubleMachBnds (initializer.cpp:933-941)
+        b.coor_x = cell_coor(h, b.i0, 0);
+        b.dh_y = cell_coor(h, b.i0, 1) - cell_coor(h, b.i0 + b.offset, 1);
+    }
+    (side == 0 ? h->bc_lo[d] : h->bc_hi[d])[lid] = b;
+    h->bc_dirty = true;
+}
+
+// Default per-line wiring of Initializer::initBnds (initializer.cpp:743-870):
+// the low end reads from the first cell with +stride (calOffset), the high end
+// from the last cell with -stride (calOffsetInverse).
+void wire_defaults(cfd_handle *h)
+{
+    for (int d = 0; d < h->dim; d++) {
+        long long nl = nlines(h, d);
+        h->bc_lo[d].assign(nl, BcLine{});
+        h->bc_hi[d].assign(nl, BcLine{});
+        int t0, t1;
+        transverse_axes(d, t0, t1);
+        for (long long lid = 0; lid < nl; lid++) {
+            long long a = lid % h->cfg.n[t0], bb = lid / h->cfg.n[t0];
+            long long base = a * h->stride[t0] + bb * h->stride[t1];
+            long long last = base + (long long)(h->cfg.n[d] - 1) * h->stride[d];
+            set_line(h, d, lid, 0, h->cfg.bc[d][0], base, (int)h->stride[d], -1);
+            set_line(h, d, lid, 1, h->cfg.bc[d][1], last, -(int)h->stride[d], -1);
+        }
+    }
+}
+
+int sync_bc(cfd_handle *h)
+{
+    if (!h->bc_dirty) return CFD_OK;
+    for (int d = 0; d < h->dim; d++) {
+        size_t bytes = h->bc_lo[d].size() * sizeof(BcLine);
+        CFD_CUDA(h, cudaMemcpyAsync(h->d_bclo[d], h->bc_lo[d].data(), bytes, cudaMemcpyHostToDevice, h->stream));
+        CFD_CUDA(h, cudaMemcpyAsync(h->d_bchi[d], h->bc_hi[d].data(), bytes, cudaMemcpyHostToDevice, h->stream));
+    }
+    if (!h->bc_vals.empty()) {
+        size_t bytes = h->bc_vals.size() * sizeof(double);
+        if (bytes > h->d_bcvals_cap) {
+            if (h->d_bcvals) cudaFree(h->d_bcvals);
+            h->d_bcvals = nullptr;
+            CFD_CUDA(h, cudaMalloc(&h->d_bcvals, bytes));
+            h->d_bcvals_cap = bytes;
+        }
+        CFD_CUDA(h, cudaMemcpyAsync(h->d_bcvals, h->bc_vals.data(), bytes, cudaMemcpyHostToDevice, h->stream));
+    }
+    // the host tables may change after this call returns
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->bc_dirty = false;
+    return CFD_OK;
+}
+
+int grid_for(long long n)
+{
+    long long g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+int launch_aos_to_soa(cfd_handle *h, const double *aos, double *soa)
+{
+    int g = grid_for(h->ncell);
+    if (h->nv == 3) aos_to_soa_kernel<3><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
+    else if (h->nv == 4) aos_to_soa_kernel<4><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
+    else aos_to_soa_kernel<5><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
+    CFD_CUDA(h, cudaGetLastError());
+    return CFD_OK;
+}
+
+int launch_soa_to_aos(cfd_handle *h, const double *soa, double *aos, int to_prim)
+{
+    int g = grid_for(h->ncell);
+    if (h->nv == 3) soa_to_aos_kernel<3><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
+    else if (h->nv == 4) soa_to_aos_kernel<4><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
+    else soa_to_aos_kernel<5><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
+    CFD_CUDA(h, cudaGetLastError());
+    return CFD_OK;
+}
+
+SweepParams base_params(cfd_handle *h, int d)
+{
+    SweepParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.ncell = h->ncell;
+    for (int k = 0; k < 3; k++) {
+        p.n[k] = h->cfg.n[k];
+        p.stride[k] = h->stride[k];
+        p.hdir[k] = h->cfg.h[k];
+    }
+    p.h = h->cfg.h[d];
+    p.red = h->red;
+    p.err = h->err;
+    p.bc_lo = h->d_bclo[d];
+    p.bc_hi = h->d_bchi[d];
+    p.bc_vals = h->d_bcvals;
+    p.icst = h->icst;
+    p.seg_len = h->seg_len[d];
+    p.dm_u = h->dm_u;
+    p.dm_v = h->dm_v;
+    return p;
+}
+
+int sweep(cfd_handle *h, int d, const SweepParams &p)
+{
+    cudaError_t e = cfd::launch_sweep_any(h->strict, h->nv, h->fam, d, h->cfg.flux_method, p, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "sweep kernel launch");
+    return CFD_OK;
+}
+
+// One RHS evaluation into h->rhs (all directions, x first as rhsSolve does).
+int rhs_all(cfd_handle *h, const double *u, double t)
+{
+    for (int d = 0; d < h->dim; d++) {
+        SweepParams p = base_params(h, d);
+        p.u = u;
+        p.rhs = h->rhs;
+        p.mode = cfd::MODE_WRITE;
+        p.first = (d == 0);
+        p.t = t;
+        int rc = sweep(h, d, p);
+        if (rc) return rc;
+    }
+    return CFD_OK;
+}
+
+// One RK stage: RHS of uin, then uout = combination (blockSolver.cpp:51-86).
+int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, double *uout, double A, double Bdt,
+             double C, double t, bool reduce)
+{
+    for (int d = 0; d < h->dim; d++) {
+        SweepParams p = base_params(h, d);
+        p.u = uin;
+        p.u0 = u0;
+        p.rhs = h->rhs;
+        p.u_out = uout;
+        bool last = (d == h->dim - 1);
+        p.mode = last ? cfd::MODE_RK : cfd::MODE_WRITE;
+        p.first = (d == 0);
+        p.rk_stage = stage;
+        p.rkA = A;
+        p.rkBdt = Bdt;
+        p.rkC = C;
+        p.want_reduce = (reduce && last) ? 1 : 0;
+        p.t = t;
+        int rc = sweep(h, d, p);
+        if (rc) return rc;
+    }
+    return CFD_OK;
+}
+
+int default_seg_len(const cfd_handle *h, int d)
+{
+    int n = h->cfg.n[d];
+    int S = (h->dim == 1) ? 128 : (d == 0 ? 64 : 8);
+    int W = (h->dim == 1) ? 1 : (d == 0 ? 4 : 32);
+    int t0, t1;
+    transverse_axes(d, t0, t1);
+    long long blocks_per_seg = (long long)((h->cfg.n[t0] + W - 1) / W) * h->cfg.n[t1];
+    const long long target = 148LL * 2 * 6;  // about six waves of two CTAs per SM
+    int seg = n;
+    while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
+    return seg;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *cfd_version(void) { return "cfdgpu 0.1 (sm_100a)"; }
+
+void cfd_config_default(cfd_config *c)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->dim = 2;
+    c->n[0] = c->n[1] = 200;
+    c->n[2] = 1;
+    c->h[0] = c->h[1] = c->h[2] = 0.3 / 200;
+    c->n_ghost = kGhost;
+    c->gamma = 1.4;
+    c->inter_method = 2;   // WCNS5
+    c->flux_method = CFD_FLUX_HLLC;
+    c->diff_method = CFD_DIFF_MND6;
+    c->precision = CFD_PREC_FP64;
+    c->strict = 0;
+    for (int d = 0; d < 3; d++) c->bc[d][0] = c->bc[d][1] = CFD_BND_SUPERSONICOUTLET;
+    c->device = 0;
+}
+
+int cfd_create(const cfd_config *cfg, cfd_handle **out)
+{
+    if (!cfg || !out) return CFD_ERR_CONFIG;
+    *out = nullptr;
+    if (cfg->dim < 1 || cfg->dim > 3) return CFD_ERR_CONFIG;
+    if (cfg->n_ghost != kGhost) return CFD_ERR_UNSUPPORTED;
+    if (cfg->gamma != 1.4) return CFD_ERR_UNSUPPORTED;
+    if (cfg->diff_method != CFD_DIFF_MND6) return CFD_ERR_UNSUPPORTED;
+    if (cfg->flux_method != CFD_FLUX_HLLC && cfg->flux_method != CFD_FLUX_ROE) return CFD_ERR_CONFIG;
+    if (cfg->precision != CFD_PREC_FP64) return CFD_ERR_UNSUPPORTED;
+    for (int d = 0; d < 3; d++) {
+        if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
+        if (d >= cfg->dim && cfg->n[d] != 1) return CFD_ERR_CONFIG;
+    }
+    InterMap im = map_inter_method(cfg->inter_method, cfg->dim);
+    if (!im.ok) return CFD_ERR_UNSUPPORTED;
+
+    cfd_handle *h = new cfd_handle();
+    h->cfg = *cfg;
+    h->dim = cfg->dim;
+    h->nv = cfg->dim + 2;
+    h->ncell = (long long)cfg->n[0] * cfg->n[1] * cfg->n[2];
+    h->stride[0] = 1;
+    h->stride[1] = cfg->n[0];
+    h->stride[2] = (long long)cfg->n[0] * cfg->n[1];
+    h->fam = im.fam;
+    h->icst = im.c;
+    h->strict = cfg->strict != 0;
+    h->dm_u = 8.25 * std::cos(M_PI / 6);
+    h->dm_v = -8.25 * std::sin(M_PI / 6);
+    for (int d = 0; d < 3; d++) {
+        h->seg_len[d] = 1;
+        if (d < h->dim) h->seg_len[d] = cfg->seg_len[d] > 0 ? cfg->seg_len[d] : default_seg_len(h, d);
+    }
+
+    auto bail = [&](cudaError_t e, const char *what) {
+        int code = (e == cudaErrorMemoryAllocation) ? CFD_ERR_NOMEM : CFD_ERR_CUDA;
+        fprintf(stderr, "cfd_create: %s: %s\n", what, cudaGetErrorString(e));
+        cfd_destroy(h);
+        return code;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(cfg->device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    size_t bytes = sizeof(double) * h->ncell * h->nv;
+    for (int k = 0; k < 3; k++)
+        if ((e = cudaMalloc(&h->u[k], bytes)) != cudaSuccess) return bail(e, "state");
+    if ((e = cudaMalloc(&h->rhs, bytes)) != cudaSuccess) return bail(e, "rhs");
+    if ((e = cudaMalloc(&h->stage, bytes)) != cudaSuccess) return bail(e, "staging");
+    if ((e = cudaMalloc(&h->red, 8 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "reductions");
+    if ((e = cudaMalloc(&h->err, sizeof(unsigned))) != cudaSuccess) return bail(e, "error word");
+    if ((e = cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream)) != cudaSuccess) return bail(e, "memset");
+    for (int k = 0; k < 3; k++)
+        if ((e = cudaMemsetAsync(h->u[k], 0, bytes, h->stream)) != cudaSuccess) return bail(e, "memset");
+    for (int d = 0; d < h->dim; d++) {
+        size_t lb = sizeof(BcLine) * (h->ncell / cfg->n[d]);
+        if ((e = cudaMalloc(&h->d_bclo[d], lb)) != cudaSuccess) return bail(e, "bc tables");
+        if ((e = cudaMalloc(&h->d_bchi[d], lb)) != cudaSuccess) return bail(e, "bc tables");
+    }
+    wire_defaults(h);
+    if (sync_bc(h) != CFD_OK) {
+        fprintf(stderr, "cfd_create: %s\n", h->msg.c_str());
+        cfd_destroy(h);
+        return CFD_ERR_CUDA;
+    }
+    *out = h;
+    return CFD_OK;
+}
+
+void cfd_destroy(cfd_handle *h)
+{
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int k = 0; k < 3; k++) cudaFree(h->u[k]);
+    cudaFree(h->rhs);
+    cudaFree(h->stage);
+    cudaFree(h->red);
+    cudaFree(h->err);
+    for (int d = 0; d < 3; d++) {
+        cudaFree(h->d_bclo[d]);
+        cudaFree(h->d_bchi[d]);
+    }
+    cudaFree(h->d_bcvals);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char *cfd_last_error(const cfd_handle *h) { return h ? h->msg.c_str() : "null handle"; }
+
+int cfd_set_line_bc(cfd_handle *h, int idim, int i, int j, int side, int bnd_type, long long i0, int offset,
+                    const double *ghost_prim)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    int d = idim - 1;
+    if (d < 0 || d >= h->dim || (side != 0 && side != 1)) return fail(h, CFD_ERR_CONFIG, "bad idim/side");
+    int t0, t1;
+    transverse_axes(d, t0, t1);
+    if (i < 0 || i >= h->cfg.n[t0] || j < 0 || j >= h->cfg.n[t1]) return fail(h, CFD_ERR_CONFIG, "line index out of range");
+    if (bnd_type != CFD_BND_PERIODIC_WRAP && (i0 < 0 || i0 >= h->ncell)) return fail(h, CFD_ERR_CONFIG, "i0 out of range");
+    if (bnd_type == CFD_BND_PERIODIC1D || (bnd_type >= CFD_BND_SYMMETRYX && bnd_type <= CFD_BND_SYMMETRYZ) ||
+        bnd_type == CFD_BND_SYMMETRY1D) {
+        long long last = i0 + (long long)(kGhost - 1) * offset;
+        if (last < 0 || last >= h->ncell) return fail(h, CFD_ERR_CONFIG, "ghost source outside the grid");
+    }
+    int slot = -1;
+    if (ghost_prim) {
+        slot = (int)(h->bc_vals.size() / (kGhost * h->nv));
+        h->bc_vals.insert(h->bc_vals.end(), ghost_prim, ghost_prim + kGhost * h->nv);
+    }
+    long long lid = i + (long long)h->cfg.n[t0] * j;
+    set_line(h, d, lid, side, bnd_type, i0, offset, slot);
+    return CFD_OK;
+}
+
+int cfd_upload_cons(cfd_handle *h, const double *aos)
+{
+    if (!h || !aos) return CFD_ERR_CONFIG;
+    size_t bytes = sizeof(double) * h->ncell * h->nv;
+    CFD_CUDA(h, cudaMemcpyAsync(h->stage, aos, bytes, cudaMemcpyHostToDevice, h->stream));
+    int rc = launch_aos_to_soa(h, h->stage, h->u[h->cur]);
+    if (rc) return rc;
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->ws_valid = false;
+    return CFD_OK;
+}
+
+int cfd_download_cons(cfd_handle *h, double *aos)
+{
+    if (!h || !aos) return CFD_ERR_CONFIG;
+    int rc = launch_soa_to_aos(h, h->u[h->cur], h->stage, 0);
+    if (rc) return rc;
+    CFD_CUDA(h, cudaMemcpyAsync(aos, h->stage, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}
+
+int cfd_download_prim(cfd_handle *h, double *aos)
+{
+    if (!h || !aos) return CFD_ERR_CONFIG;
+    int rc = launch_soa_to_aos(h, h->u[h->cur], h->stage, 1);
+    if (rc) return rc;
+    CFD_CUDA(h, cudaMemcpyAsync(aos, h->stage, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}
+
+int cfd_rhs(cfd_handle *h, double t, double *aos_rhs)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    int rc = sync_bc(h);
+    if (rc) return rc;
+    rc = rhs_all(h, h->u[h->cur], t);
+    if (rc) return rc;
+    if (aos_rhs) {
+        rc = launch_soa_to_aos(h, h->rhs, h->stage, 0);
+        if (rc) return rc;
+        CFD_CUDA(h, cudaMemcpyAsync(aos_rhs, h->stage, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToHost,
+                                    h->stream));
+    }
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}
+
+int cfd_max_dt(cfd_handle *h, double cfl, double *dt)
+{
+    if (!h || !dt) return CFD_ERR_CONFIG;
+    unsigned long long r[4];
+    if (!h->ws_valid) {
+        CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
+        int g = grid_for(h->ncell);
+        const double *u = h->u[h->cur];
+        if (h->nv == 3) wave_speed_kernel<3><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+        else if (h->nv == 4) wave_speed_kernel<4><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+        else wave_speed_kernel<5><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+        CFD_CUDA(h, cudaGetLastError());
+    }
+    CFD_CUDA(h, cudaMemcpyAsync(r, h->red, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    double lambda = 0;
+    for (int d = 0; d < h->dim; d++) {
+        double l;
+        std::memcpy(&l, &r[1 + d], sizeof(double));
+        lambda += l;
+    }
+    *dt = cfl / lambda;
+    return CFD_OK;
+}
+
+int cfd_rk3_step(cfd_handle *h, double dt, double t, double *rho_linf)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    int rc = sync_bc(h);
+    if (rc) return rc;
+    double *U0 = h->u[h->cur], *U1 = h->u[(h->cur + 1) % 3], *U2 = h->u[(h->cur + 2) % 3];
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+    // stage times follow info->t in RK3_SSP: t, t + dt, (t + dt) - dt/2
+    double t1 = t, t2 = t + dt, t3 = t2 - dt / 2;
+    if ((rc = rk_stage(h, 1, U0, U0, U1, 1.0, dt, 0.0, t1, false))) return rc;
+    if ((rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.25 * dt, 0.25, t2, false))) return rc;
+    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
+    if ((rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 2.0 / 3.0 * dt, 2.0 / 3.0, t3, true))) return rc;
+    h->cur = (h->cur + 1) % 3;
+    h->ws_valid = true;
+    unsigned long long r0;
+    unsigned err;
+    CFD_CUDA(h, cudaMemcpyAsync(&r0, h->red, sizeof(r0), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (rho_linf) std::memcpy(rho_linf, &r0, sizeof(double));
+    if (err & cfd::ERR_NONFINITE) return fail(h, CFD_ERR_NONFINITE, "non-finite value in the state after an RK3 step");
+    if (err & cfd::ERR_NEGATIVE) return fail(h, CFD_ERR_NEGATIVE_STATE, "density or pressure <= 0 after an RK3 step");
+    return CFD_OK;
+}
+
+int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_steps, double *t, int *nsteps,
+            double *dts, double *linf)
+{
+    if (!h || !t || !nsteps) return CFD_ERR_CONFIG;
+    // stepsLoopCFL (blockSolver.cpp:170-235), one host round trip per step.
+    int step = 0, k = 0;
+    double outputT = 0.0;
+    int rc = CFD_OK;
+    while (step < end_step && k < max_steps) {
+        double dt;
+        if ((rc = cfd_max_dt(h, cfl, &dt))) return rc;
+        if (outputT + dt > output_dt) {
+            dt = output_dt - outputT;
+            outputT = 0.0;
+            step++;
+        } else
+            outputT += dt;
+        double l = 0.0;
+        rc = cfd_rk3_step(h, dt, *t, &l);
+        // BlockSolver::solve: RK3_SSP moves t by +dt, -dt/2, -dt/2, then t += dt
+        *t = (((*t + dt) - dt / 2) - dt / 2) + dt;
+        if (dts) dts[k] = dt;
+        if (linf) linf[k] = l;
+        k++;
+        if (rc) break;
+    }
+    *nsteps = k;
+    return rc;
+}
+
+int cfd_device_state(cfd_handle *h, double **state, long long *ncell, void **stream)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    if (state) *state = h->u[h->cur];
+    if (ncell) *ncell = h->ncell;
+    if (stream) *stream = (void *)h->stream;
+    return CFD_OK;
+}
+
+int cfd_set_state_device(cfd_handle *h, const double *soa_dev)
+{
+    if (!h || !soa_dev) return CFD_ERR_CONFIG;
+    CFD_CUDA(h, cudaMemcpyAsync(h->u[h->cur], soa_dev, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToDevice,
+                                h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->ws_valid = false;
+    return CFD_OK;
+}
+
+int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double *out)
+{
+    (void)strict;
+    InterMap im = map_inter_method(inter_method, 2);
+    if (!im.ok) return CFD_ERR_UNSUPPORTED;
+    if (n <= 0) return CFD_OK;
+    double *dq = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dq, sizeof(double) * 5 * n) != cudaSuccess) return CFD_ERR_NOMEM;
+    if (cudaMalloc(&dout, sizeof(double) * n) != cudaSuccess) { cudaFree(dq); return CFD_ERR_NOMEM; }
+    cudaMemcpy(dq, q, sizeof(double) * 5 * n, cudaMemcpyHostToDevice);
+    int g = (n + 255) / 256;
+    switch (im.fam) {
+    case cfd::FAM_WCNS5: eval_inter5_kernel<cfd::FAM_WCNS5><<<g, 256>>>(dq, n, im.c, dout); break;
+    case cfd::FAM_WENOZ: eval_inter5_kernel<cfd::FAM_WENOZ><<<g, 256>>>(dq, n, im.c, dout); break;
+    case cfd::FAM_TENOZ: eval_inter5_kernel<cfd::FAM_TENOZ><<<g, 256>>>(dq, n, im.c, dout); break;
+    case cfd::FAM_TENOCONG: eval_inter5_kernel<cfd::FAM_TENOCONG><<<g, 256>>>(dq, n, im.c, dout); break;
+    default: eval_inter5_kernel<cfd::FAM_MUSCL><<<g, 256>>>(dq, n, im.c, dout); break;
+    }
+    cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dq);
+    cudaFree(dout);
+    return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
+}
+
+int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr, int n, double *out)
+{
+    (void)strict;
+    if (dim < 1 || dim > 3 || ax < 0 || ax >= dim) return CFD_ERR_CONFIG;
+    if (n <= 0) return CFD_OK;
+    int nv = dim + 2;
+    double *din = nullptr, *dout = nullptr;
+    if (cudaMalloc(&din, sizeof(double) * 2 * nv * n) != cudaSuccess) return CFD_ERR_NOMEM;
+    if (cudaMalloc(&dout, sizeof(double) * nv * n) != cudaSuccess) { cudaFree(din); return CFD_ERR_NOMEM; }
+    cudaMemcpy(din, lr, sizeof(double) * 2 * nv * n, cudaMemcpyHostToDevice);
+    int g = (n + 255) / 256;
+    bool hllc = flux_method == CFD_FLUX_HLLC;
+#define CFD_EF(NV, AX)                                                                                   \
+    if (nv == NV && ax == AX) {                                                                          \
+        if (hllc) eval_flux_kernel<NV, AX, cfd::FLUX_HLLC><<<g, 256>>>(din, n, dout);                   \
+        else eval_flux_kernel<NV, AX, cfd::FLUX_ROE><<<g, 256>>>(din, n, dout);                         \
+    }
+    CFD_EF(3, 0) CFD_EF(4, 0) CFD_EF(4, 1) CFD_EF(5, 0) CFD_EF(5, 1) CFD_EF(5, 2)
+#undef CFD_EF
+    cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * nv * n, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(dout);
+    return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
+}
+
+} // extern "C"

@@ -1,0 +1,745 @@
+// Pointwise arithmetic of the zone_FD right-hand side, written for sm_100a.
+//
+// Every function keeps the reference's operation order term by term, so that a
+// translation unit compiled with --fmad=false reproduces the reference's FP64
+// results bit for bit (the reference is built for generic x86-64 without FMA
+// contraction). Translation units compiled with --fmad=true get contracted
+// FMAs and, where CFD_FAST is defined, a few algebraic rewrites that trade the
+// last ulp for fewer divisions; those are marked "fast path".
+//
+// Layout conventions: prim = (rho, u, v[, w], p), cons = (rho, rho u, rho v
+// [, rho w], rho E); NV = 3 (1D), 4 (2D), 5 (3D). AX is the sweep axis
+// (0 = x, 1 = y, 2 = z); the face normal is the unit vector along AX.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#ifndef CFD_HD
+#define CFD_HD __host__ __device__ __forceinline__
+#endif
+
+namespace cfd {
+
+// zone_FD/src/include/macro.hpp:28 (#define GAMMA 1.4)
+constexpr double kGamma = 1.4;
+
+// ---------------------------------------------------------------------------
+// Five-point interpolators (zone_FD/src/include/interScheme.hpp).
+// q0..q4 are the five upwind-ordered point values; the result is the value at
+// the face between q2 and q3.
+// ---------------------------------------------------------------------------
+
+// Smoothness indicators shared by every WCNS/TENO variant
+// (interScheme.hpp:21-28, repeated in each variant).
+CFD_HD void smoothness3(double q0, double q1, double q2, double q3, double q4,
+                        double &b0, double &b1, double &b2)
+{
+    double a, b;
+    a = 1.0 * q0 - 2.0 * q1 + 1.0 * q2;
+    b = 1.0 * q0 - 4.0 * q1 + 3.0 * q2;
+    b0 = 1.0 / 1.0 * (a * a) + 1.0 / 4.0 * (b * b);
+    a = 1.0 * q1 - 2.0 * q2 + 1.0 * q3;
+    b = 1.0 * q1 + 0.0 * q2 - 1.0 * q3;
+    b1 = 1.0 / 1.0 * (a * a) + 1.0 / 4.0 * (b * b);
+    a = 1.0 * q2 - 2.0 * q3 + 1.0 * q4;
+    b = 3.0 * q2 - 4.0 * q3 + 1.0 * q4;
+    b2 = 1.0 / 1.0 * (a * a) + 1.0 / 4.0 * (b * b);
+}
+
+// The three third-order candidate values (interScheme.hpp:31-33).
+CFD_HD void candidates3(double q0, double q1, double q2, double q3, double q4,
+                        double &u0, double &u1, double &u2)
+{
+    u0 = 3.0 / 8.0 * q0 - 5.0 / 4.0 * q1 + 15.0 / 8.0 * q2;
+    u1 = -1.0 / 8.0 * q1 + 3.0 / 4.0 * q2 + 3.0 / 8.0 * q3;
+    u2 = 3.0 / 8.0 * q2 + 3.0 / 4.0 * q3 - 1.0 / 8.0 * q4;
+}
+
+// The eight fixed stencils selected by a TENO flag word (bit k set = stencil k
+// cut off), interScheme.hpp:445-480 (identical in every TENO variant).
+CFD_HD double teno_select(unsigned flag, double q0, double q1, double q2, double q3, double q4)
+{
+    switch (flag) {
+    case 0: return 3.0 / 128.0 * q0 - 5.0 / 32.0 * q1 + 45.0 / 64.0 * q2 + 15.0 / 32.0 * q3 - 5.0 / 128.0 * q4;
+    case 1: return -1.0 / 16.0 * q1 + 9.0 / 16.0 * q2 + 9.0 / 16.0 * q3 - 1.0 / 16.0 * q4;
+    case 2:
+    case 3: return 3.0 / 8.0 * q2 + 3.0 / 4.0 * q3 - 1.0 / 8.0 * q4;
+    case 4: return 1.0 / 16.0 * q0 - 5.0 / 16.0 * q1 + 15.0 / 16.0 * q2 + 5.0 / 16.0 * q3;
+    case 5: return -1.0 / 8.0 * q1 + 3.0 / 4.0 * q2 + 3.0 / 8.0 * q3;
+    case 6: return 3.0 / 8.0 * q0 - 5.0 / 4.0 * q1 + 15.0 / 8.0 * q2;
+    default: return q2;
+    }
+}
+
+// Interpolator families. Each selector entry of the reference maps onto one
+// family plus a runtime constant (InterSpec::c).
+enum InterFamily : int {
+    FAM_WCNS5 = 0,   // weno5_JSchen                       interScheme.hpp:17-45
+    FAM_WENOZ = 1,   // weno5_Z                            interScheme.hpp:85-114
+    FAM_TENOZ = 2,   // Teno5_Z / ZCT4 / ZCT7 / congTcns5_ZCT5 / ZCT10 / new_Teno5_Z
+                     //   (c = cutoff factor 1e-5, 1e-4, 1e-7, 1e-5, 1e-10, 1e-5)
+    FAM_TENOCONG = 3,// Teno5_CongZ / CongZCT4 / CongZCT7 / new_Teno5_CongZ (c = CT)
+    FAM_MUSCL = 4,   // musclIn5 (minmod on q1..q3)        interScheme.hpp:1386-1406
+};
+
+template <int FAM>
+CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, double c)
+{
+    if constexpr (FAM == FAM_WCNS5) {
+        // weno5_JSchen: omega_k = gamma_k / (eps + beta_k)^2, eps = 1e-6.
+        const double eps = 1e-6;
+        double b0, b1, b2, u0, u1, u2;
+        smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
+        candidates3(q0, q1, q2, q3, q4, u0, u1, u2);
+#if defined(CFD_FAST)
+        // fast path: one division instead of four. With s_k = eps + beta_k,
+        // sum_k g_k u_k / s_k^2 / sum_k g_k / s_k^2 equals the same sums with
+        // every term multiplied by prod_k s_k^2, i.e. weights g_k * prod_{j!=k} s_j^2.
+        double s0 = eps + b0, s1 = eps + b1, s2 = eps + b2;
+        s0 *= s0; s1 *= s1; s2 *= s2;
+        double w0 = (1.0 / 16.0) * (s1 * s2), w1 = (5.0 / 8.0) * (s0 * s2), w2 = (5.0 / 16.0) * (s0 * s1);
+        return (w0 * u0 + w1 * u1 + w2 * u2) / (w0 + w1 + w2);
+#else
+        double s;
+        s = eps + b0; b0 = (1.0 / 16.0) / (s * s);
+        s = eps + b1; b1 = (5.0 / 8.0) / (s * s);
+        s = eps + b2; b2 = (5.0 / 16.0) / (s * s);
+        double sumbeta = 0.0, result = 0.0;
+        sumbeta += b0; sumbeta += b1; sumbeta += b2;
+        result += b0 * u0; result += b1 * u1; result += b2 * u2;
+        return result / sumbeta;
+#endif
+    } else if constexpr (FAM == FAM_WENOZ) {
+        // weno5_Z: omega_k = gamma_k (1 + (tau / (beta_k + eps))^2), eps = 1e-40.
+        const double eps = 1e-40;
+        double b0, b1, b2, u0, u1, u2;
+        smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
+        candidates3(q0, q1, q2, q3, q4, u0, u1, u2);
+        double tau = fabs(b2 - b0), x;
+        x = tau / (b0 + eps); b0 = (1.0 / 16.0) * (1.0 + x * x);
+        x = tau / (b1 + eps); b1 = (5.0 / 8.0) * (1.0 + x * x);
+        x = tau / (b2 + eps); b2 = (5.0 / 16.0) * (1.0 + x * x);
+        double sumbeta = 0.0, result = 0.0;
+        sumbeta += b0; sumbeta += b1; sumbeta += b2;
+        result += b0 * u0; result += b1 * u1; result += b2 * u2;
+        return result / sumbeta;
+    } else if constexpr (FAM == FAM_TENOZ) {
+        // TENO5 with the Z-type measure (1 + tau/(beta_k + eps))^6 and the
+        // cutoff measure_k < c * sum_j measure_j (Teno5_Z: interScheme.hpp:384-452).
+        const double eps = 1e-40;
+        double b0, b1, b2;
+        smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
+        double tau = fabs(b2 - b0), t;
+        t = 1.0 + tau / (b0 + eps); t *= t; b0 = t * t * t;
+        t = 1.0 + tau / (b1 + eps); t *= t; b1 = t * t * t;
+        t = 1.0 + tau / (b2 + eps); t *= t; b2 = t * t * t;
+        double sumbeta = 0.0;
+        sumbeta += b0; sumbeta += b1; sumbeta += b2;
+        double CT = c * sumbeta;
+        unsigned flag = 0;
+        if (b0 < CT) flag += 1;
+        if (b1 < CT) flag += 2;
+        if (b2 < CT) flag += 4;
+        return teno_select(flag, q0, q1, q2, q3, q4);
+    } else if constexpr (FAM == FAM_TENOCONG) {
+        // Cross-multiplied TENO cutoff of Teno5_CongZ (interScheme.hpp:494-584):
+        // stencil k is cut when tau*beta_min < (CT*tau - (1-CT)*beta_min) * beta_k.
+        double b0, b1, b2;
+        smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
+        // std::min_element: first index of the smallest value.
+        double bmin = b0;
+        if (b1 < bmin) bmin = b1;
+        if (b2 < bmin) bmin = b2;
+        const double CT = c, CT_1 = 1.0 - c;
+        double tau = fabs(b2 - b0);
+        double rr = CT * tau - CT_1 * bmin;
+        double ll = tau * bmin;
+        unsigned flag = 0;
+        if (ll < rr * b0) flag += 1;
+        if (ll < rr * b1) flag += 2;
+        if (ll < rr * b2) flag += 4;
+        return teno_select(flag, q0, q1, q2, q3, q4);
+    } else {
+        // musclIn5: minmod limited slope on (q1, q2, q3).
+        double deltam = q2 - q1, deltap = q3 - q2, delta;
+        const double beta = 1.0;
+        // std::max(a,b) = (a < b) ? b : a ; std::min(a,b) = (b < a) ? b : a
+        auto smax = [](double a, double b) { return (a < b) ? b : a; };
+        auto smin = [](double a, double b) { return (b < a) ? b : a; };
+        if (deltap > 0) {
+            delta = smax(0.0, smax(smin(beta * deltam, deltap), smin(deltam, beta * deltap)));
+        } else {
+            delta = smin(0.0, smin(smax(beta * deltam, deltap), smax(deltam, beta * deltap)));
+        }
+        return q2 + delta * 0.5;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// cons -> prim as Equation::consToPrimEuler{1D,2D} (equation.cpp:37-93); the
+// 3D form adds w the same way.
+// ---------------------------------------------------------------------------
+template <int NV>
+CFD_HD void cons_to_prim(const double *c, double *p)
+{
+    const double gamma = kGamma;
+    if constexpr (NV == 3) {
+        double r = c[0], ru = c[1], rE = c[2];
+        double u = ru / r;
+        double E = rE / r;
+        double e = -u * u / 2 + E;
+        double RT = (gamma - 1) * e;
+        p[0] = r; p[1] = u; p[2] = r * RT;
+    } else if constexpr (NV == 4) {
+        double r = c[0], ru = c[1], rv = c[2], rE = c[3];
+        double u = ru / r, v = rv / r, E = rE / r;
+        double q2 = (u * u + v * v) / 2;
+        double e = -q2 + E;
+        double RT = (gamma - 1) * e;
+        p[0] = r; p[1] = u; p[2] = v; p[3] = r * RT;
+    } else {
+        double r = c[0], ru = c[1], rv = c[2], rw = c[3], rE = c[4];
+        double u = ru / r, v = rv / r, w = rw / r, E = rE / r;
+        double q2 = (u * u + v * v + w * w) / 2;
+        double e = -q2 + E;
+        double RT = (gamma - 1) * e;
+        p[0] = r; p[1] = u; p[2] = v; p[3] = w; p[4] = r * RT;
+    }
+}
+
+// prim -> cons as the eigensystem's primToCons/primToChar prologue
+// (eigenSystem.cpp:91-93 for 2D, :254-256 for 1D).
+template <int NV>
+CFD_HD void prim_to_cons(const double *p, double *c)
+{
+    const double gamma = kGamma;
+    if constexpr (NV == 3) {
+        double rt = p[0], ut = p[1], pt = p[2];
+        double ekt = (ut * ut) / 2;
+        c[0] = rt; c[1] = rt * ut; c[2] = pt / (gamma - 1) + rt * ekt;
+    } else if constexpr (NV == 4) {
+        double rt = p[0], ut = p[1], vt = p[2], pt = p[3];
+        double ekt = (ut * ut + vt * vt) / 2;
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = pt / (gamma - 1) + rt * ekt;
+    } else {
+        double rt = p[0], ut = p[1], vt = p[2], wt = p[3], pt = p[4];
+        double ekt = (ut * ut + vt * vt + wt * wt) / 2;
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = pt / (gamma - 1) + rt * ekt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Roe-averaged characteristic system.
+// 1D: eigensystemEuler1D (eigenSystem.cpp:217-323).
+// 2D: eigensystemEuler2D (eigenSystem.cpp:13-213), normal = unit vector AX.
+// 3D: the 2D system extended by a second shear wave (this library's own
+//     extension; the reference has no 3D Euler path). For a field with w = 0
+//     that does not vary along z, it reduces to the 2D system value for value.
+// ---------------------------------------------------------------------------
+template <int NV, int AX>
+struct Eigen {
+    double L[NV][NV];  // rows = left eigenvectors (char = L * cons)
+    double R[NV][NV];  // R[row][col]: cons = R * char
+
+    CFD_HD Eigen(const double *pl, const double *pr)
+    {
+        const double gamma = kGamma;
+        if constexpr (NV == 3) {
+            double rl = pl[0], ul = pl[1], pL = pl[2];
+            double rr = pr[0], ur = pr[1], pR = pr[2];
+            double HL = (ul * ul) / 2 + pL / rl * gamma / (gamma - 1);
+            double HR = (ur * ur) / 2 + pR / rr * gamma / (gamma - 1);
+            double coef1 = sqrt(rl), coef2 = sqrt(rr);
+            double divisor = 1.0 / (coef1 + coef2);
+            double u = (coef1 * ul + coef2 * ur) * divisor;
+            double ht = (coef1 * HL + coef2 * HR) * divisor;
+            double ek = (u * u) / 2;
+            double h = ht - ek;
+            double c = sqrt((gamma - 1) * h);
+            double g1 = gamma - 1;
+            double le[9] = {ht + c * (u - c) / g1, -u - c / g1, 1.0,
+                            -2.0 * ht + 4.0 * c * c / g1, 2.0 * u, -2.0,
+                            ht - c * (u + c) / g1, -u + c / g1, 1.0};
+            double f = 0.5 * g1 / (c * c);
+            for (int i = 0; i < 9; i++) L[i / 3][i % 3] = le[i] * f;
+            double re[9] = {1.0, 1.0, 1.0, u - c, u, u + c, ht - u * c, 0.5 * u * u, ht + u * c};
+            for (int i = 0; i < 9; i++) R[i / 3][i % 3] = re[i];
+        } else {
+            constexpr int D = (NV == 4) ? 2 : 3;
+            double vl[3] = {pl[1], pl[2], D == 3 ? pl[3] : 0.0};
+            double vr[3] = {pr[1], pr[2], D == 3 ? pr[3] : 0.0};
+            double rl = pl[0], rr = pr[0], pL = pl[NV - 1], pR = pr[NV - 1];
+            double HL, HR;
+            if constexpr (D == 2) {
+                HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pL / rl * gamma / (gamma - 1);
+                HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pR / rr * gamma / (gamma - 1);
+            } else {
+                HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pL / rl * gamma / (gamma - 1);
+                HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pR / rr * gamma / (gamma - 1);
+            }
+            double coef1 = sqrt(rl), coef2 = sqrt(rr);
+            double divisor = 1.0 / (coef1 + coef2);
+            double u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
+            double v = (coef1 * vl[1] + coef2 * vr[1]) * divisor;
+            double w = (D == 3) ? (coef1 * vl[2] + coef2 * vr[2]) * divisor : 0.0;
+            double ht = (coef1 * HL + coef2 * HR) * divisor;
+            const double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0, nz = (AX == 2) ? 1.0 : 0.0;
+            double Vn, ek;
+            if constexpr (D == 2) {
+                Vn = nx * u + ny * v;
+                ek = (u * u + v * v) / 2;
+            } else {
+                Vn = nx * u + ny * v + nz * w;
+                ek = (u * u + v * v + w * w) / 2;
+            }
+            double h = ht - ek;
+            double c = sqrt((gamma - 1) * h);
+            // rows: 0 shear (tangent t1), 1 entropy, 2 acoustic (Vn - c), 3 acoustic (Vn + c)
+            // [, 4 shear (tangent t2) in 3D]
+            // column order in L rows and R rows: rho, rho u, rho v, [rho w,] rho E
+            constexpr int E = NV - 1;
+#if defined(CFD_FAST)
+            // fast path: share the reciprocals of c and h.
+            const double ic = 1.0 / c, ih = 1.0 / h;
+#define CFD_DIV_C(a) ((a) * ic)
+#define CFD_DIV_H(a) ((a) * ih)
+#else
+#define CFD_DIV_C(a) ((a) / c)
+#define CFD_DIV_H(a) ((a) / h)
+#endif
+            if constexpr (AX != 2) {
+                L[0][0] = (-ny * u + nx * v); L[0][1] = ny; L[0][2] = (-nx);
+            } else {
+                L[0][0] = -u; L[0][1] = 1.0; L[0][2] = 0.0;
+            }
+            if constexpr (D == 3) L[0][3] = 0.0;
+            L[0][E] = 0;
+            L[1][0] = (h - ek); L[1][1] = u; L[1][2] = v;
+            if constexpr (D == 3) L[1][3] = w;
+            L[1][E] = -1.0;
+            L[2][0] = (CFD_DIV_C(Vn) + CFD_DIV_H(ek)) / 2;
+            L[2][1] = (CFD_DIV_C(-nx) - CFD_DIV_H(u)) / 2;
+            L[2][2] = (CFD_DIV_C(-ny) - CFD_DIV_H(v)) / 2;
+            if constexpr (D == 3) L[2][3] = (CFD_DIV_C(-nz) - CFD_DIV_H(w)) / 2;
+            L[2][E] = 1.0 / (2.0 * h);
+            L[3][0] = (CFD_DIV_C(-Vn) + CFD_DIV_H(ek)) / 2;
+            L[3][1] = (CFD_DIV_C(nx) - CFD_DIV_H(u)) / 2;
+            L[3][2] = (CFD_DIV_C(ny) - CFD_DIV_H(v)) / 2;
+            if constexpr (D == 3) L[3][3] = (CFD_DIV_C(nz) - CFD_DIV_H(w)) / 2;
+            L[3][E] = 1.0 / (2.0 * h);
+            if constexpr (D == 3) {
+                if constexpr (AX != 2) {
+                    L[4][0] = -w; L[4][1] = 0.0; L[4][2] = 0.0; L[4][3] = 1.0; L[4][4] = 0.0;
+                } else {
+                    L[4][0] = -v; L[4][1] = 0.0; L[4][2] = 1.0; L[4][3] = 0.0; L[4][4] = 0.0;
+                }
+            }
+            // right eigenvectors, stored by row of cons
+            if constexpr (AX != 2) {
+                R[0][0] = 0; R[1][0] = ny; R[2][0] = -nx; R[E][0] = ny * u - nx * v;
+                if constexpr (D == 3) R[3][0] = 0.0;
+            } else {
+                R[0][0] = 0; R[1][0] = 1.0; R[2][0] = 0.0; R[3][0] = 0.0; R[E][0] = u;
+            }
+            R[0][1] = 1.0 / h; R[1][1] = CFD_DIV_H(u); R[2][1] = CFD_DIV_H(v); R[E][1] = CFD_DIV_H(ek);
+            if constexpr (D == 3) R[3][1] = CFD_DIV_H(w);
+            R[0][2] = 1; R[1][2] = u - nx * c; R[2][2] = v - ny * c; R[E][2] = h + ek - Vn * c;
+            if constexpr (D == 3) R[3][2] = w - nz * c;
+            R[0][3] = 1; R[1][3] = u + nx * c; R[2][3] = v + ny * c; R[E][3] = h + ek + Vn * c;
+            if constexpr (D == 3) R[3][3] = w + nz * c;
+            if constexpr (D == 3) {
+                if constexpr (AX != 2) {
+                    R[0][4] = 0.0; R[1][4] = 0.0; R[2][4] = 0.0; R[3][4] = 1.0; R[4][4] = w;
+                } else {
+                    R[0][4] = 0.0; R[1][4] = 0.0; R[2][4] = 1.0; R[3][4] = 0.0; R[4][4] = v;
+                }
+            }
+#undef CFD_DIV_C
+#undef CFD_DIV_H
+        }
+    }
+
+    // char = L * cons with the reference's summation order
+    // (1D: rt L0 + rut L1 + ret L2, eigenSystem.cpp:260-264;
+    //  2D: rut L1 + rvt L2 + ret L3 + rt L0, eigenSystem.cpp:97-106;
+    //  3D: rut L1 + rvt L2 + rwt L3 + ret L4 + rt L0).
+    CFD_HD double project(int k, const double *cs) const
+    {
+        if constexpr (NV == 3) {
+            return cs[0] * L[k][0] + cs[1] * L[k][1] + cs[2] * L[k][2];
+        } else if constexpr (NV == 4) {
+            return cs[1] * L[k][1] + cs[2] * L[k][2] + cs[3] * L[k][3] + cs[0] * L[k][0];
+        } else {
+            return cs[1] * L[k][1] + cs[2] * L[k][2] + cs[3] * L[k][3] + cs[4] * L[k][4] + cs[0] * L[k][0];
+        }
+    }
+
+    // cons = R * char with the reference's summation order
+    // (1D: ch1 R0 + ch2 R1 + ch3 R2, eigenSystem.cpp:300-302;
+    //  2D: ch3 R2 + ch4 R3 + ch2 R1 + ch1 R0, eigenSystem.cpp:139-149;
+    //  3D: the 2D order followed by + ch5 R4).
+    CFD_HD void back(const double *ch, double *cs) const
+    {
+        for (int i = 0; i < NV; i++) {
+            if constexpr (NV == 3) {
+                cs[i] = ch[0] * R[i][0] + ch[1] * R[i][1] + ch[2] * R[i][2];
+            } else if constexpr (NV == 4) {
+                cs[i] = ch[2] * R[i][2] + ch[3] * R[i][3] + ch[1] * R[i][1] + ch[0] * R[i][0];
+            } else {
+                cs[i] = ch[2] * R[i][2] + ch[3] * R[i][3] + ch[1] * R[i][1] + ch[0] * R[i][0] + ch[4] * R[i][4];
+            }
+        }
+    }
+};
+
+// charToPrim's cons -> prim tail (2D: eigenSystem.cpp:163-167; 3D adds w).
+template <int NV>
+CFD_HD void char_cons_to_prim(const double *cs, double *p)
+{
+    const double gamma = kGamma;
+    if constexpr (NV == 3) {
+        // eigensystemEuler1D::consToPrim (eigenSystem.cpp:309-322)
+        double rt = cs[0], rut = cs[1], ret = cs[2];
+        double ut = rut / rt;
+        double ekt = (ut * ut) / 2;
+        p[0] = rt; p[1] = ut; p[2] = (gamma - 1) * (ret - rt * ekt);
+    } else if constexpr (NV == 4) {
+        double rt = cs[0], rut = cs[1], rvt = cs[2], ret = cs[3];
+        double ut = rut / rt, vt = rvt / rt;
+        double rekt = (rut * rut + rvt * rvt) / rt / 2;
+        p[0] = rt; p[1] = ut; p[2] = vt; p[3] = (gamma - 1) * (ret - rekt);
+    } else {
+        double rt = cs[0], rut = cs[1], rvt = cs[2], rwt = cs[3], ret = cs[4];
+        double ut = rut / rt, vt = rvt / rt, wt = rwt / rt;
+        double rekt = (rut * rut + rvt * rvt + rwt * rwt) / rt / 2;
+        p[0] = rt; p[1] = ut; p[2] = vt; p[3] = wt; p[4] = (gamma - 1) * (ret - rekt);
+    }
+}
+
+// variable_positive_limiter (positive_preserving.hpp:13-46) applied to the
+// density (which = 0) or to gamma * p (which = 1) of a 1D cons triple.
+CFD_HD double positive_quantity_1d(int which, const double *W)
+{
+    if (which == 0) return W[0];
+    double rho = W[0], rhou = W[1], rhoE = W[2];
+    double u = rhou / rho;
+    double ekin = 0.5 * u * u;
+    double p = (kGamma - 1) * (rhoE - rho * ekin);
+    return kGamma * p;
+}
+CFD_HD void positive_limit_1d(int which, const double *W, double *Wi)
+{
+    const double EPS = 1e-10;
+    double qi = positive_quantity_1d(which, Wi);
+    if (qi >= EPS) return;
+    double q = positive_quantity_1d(which, W);
+    if (q < EPS) {
+        for (int i = 0; i < 3; i++) Wi[i] = W[i];
+        return;
+    }
+    double theta = (EPS - q) / (qi - q);
+    for (int i = 0; i < 3; i++) Wi[i] = (1 - theta) * W[i] + theta * Wi[i];
+}
+
+// ---------------------------------------------------------------------------
+// Face reconstruction (Recon5Order{1D,2D}EulerEig::reconI,
+// reconstructor5order.hpp:233-323 and 326-429). cs6/pr6 are the re-derived
+// cons and the prim of the six stencil cells (face between cell 2 and 3).
+// Writes the left and right face prim states.
+// ---------------------------------------------------------------------------
+template <int NV, int AX, int FAM>
+CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], double icst,
+                             double *fl, double *fr)
+{
+    Eigen<NV, AX> eig(pr6[2], pr6[3]);
+    double QL[NV], QR[NV];
+    for (int k = 0; k < NV; k++) {
+        double q[6];
+        for (int j = 0; j < 6; j++) q[j] = eig.project(k, cs6[j]);
+        QL[k] = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst);
+        QR[k] = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst);
+    }
+    double cl[NV], cr[NV];
+    eig.back(QL, cl);
+    eig.back(QR, cr);
+    if constexpr (NV == 3) {
+        double consL[3], consR[3];
+        prim_to_cons<3>(pr6[2], consL);
+        prim_to_cons<3>(pr6[3], consR);
+        positive_limit_1d(0, consL, cl);
+        positive_limit_1d(0, consR, cr);
+        positive_limit_1d(1, consL, cl);
+        positive_limit_1d(1, consR, cr);
+        char_cons_to_prim<3>(cl, fl);
+        char_cons_to_prim<3>(cr, fr);
+    } else {
+        char_cons_to_prim<NV>(cl, fl);
+        char_cons_to_prim<NV>(cr, fr);
+        // crude positivity fallback (reconstructor5order.hpp:380-381), including
+        // the reference's mix of right density/pressure with left velocity.
+        if (fl[0] < 0 || fl[NV - 1] < 0) {
+            for (int i = 0; i < NV; i++) fl[i] = pr6[2][i];
+        }
+        if (fr[0] < 0 || fr[NV - 1] < 0) {
+            fr[0] = pr6[3][0];
+            for (int i = 1; i < NV - 1; i++) fr[i] = pr6[2][i];
+            fr[NV - 1] = pr6[3][NV - 1];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann fluxes.
+// ---------------------------------------------------------------------------
+enum FluxKind : int { FLUX_HLLC = 0, FLUX_ROE = 1 };
+
+// HLLCFlux1D (fluxSchemes.hpp:74-125)
+CFD_HD void hllc_1d(const double *L, const double *R, double *res)
+{
+    const double gamma = kGamma;
+    double rl = L[0], ul = L[1], pl = L[2], rr = R[0], ur = R[1], pr = R[2];
+    double HL = pl / rl * kGamma / (kGamma - 1) + (ul * ul) / 2;
+    double HR = pr / rr * kGamma / (kGamma - 1) + (ur * ur) / 2;
+    double cl = sqrt(gamma * (pl / rl));
+    double cr = sqrt(gamma * (pr / rr));
+    // std::min(ur - cr, ul - cl) and std::max(ul + cl, ur + cr)
+    double SL = ((ul - cl) < (ur - cr)) ? (ul - cl) : (ur - cr);
+    double SR = ((ul + cl) < (ur + cr)) ? (ur + cr) : (ul + cl);
+    double Sstar = ((pr - pl) + (rl * ul * (SL - ul) - rr * ur * (SR - ur))) / (rl * (SL - ul) - rr * (SR - ur));
+    if (SL >= 0) {
+        res[0] = rl * ul; res[1] = rl * ul * ul + pl; res[2] = rl * HL * ul;
+    } else if (Sstar >= 0) {
+        double pStar = pl + rl * (SL - ul) * (Sstar - ul);
+        double U[3] = {rl, rl * ul, pl / (gamma - 1) + rl * ul * ul / 2};
+        double F[3] = {rl * ul, rl * ul * ul + pl, rl * HL * ul};
+        double D[3] = {0, 1, Sstar};
+        for (int i = 0; i < 3; i++) res[i] = (Sstar * (SL * U[i] - F[i]) + SL * pStar * D[i]) / (SL - Sstar);
+    } else if (SR >= 0) {
+        double pStar = pr + rr * (SR - ur) * (Sstar - ur);
+        double U[3] = {rr, rr * ur, pr / (gamma - 1) + rr * ur * ur / 2};
+        double F[3] = {rr * ur, rr * ur * ur + pr, rr * HR * ur};
+        double D[3] = {0, 1, Sstar};
+        for (int i = 0; i < 3; i++) res[i] = (Sstar * (SR * U[i] - F[i]) + SR * pStar * D[i]) / (SR - Sstar);
+    } else {
+        res[0] = rr * ur; res[1] = rr * ur * ur + pr; res[2] = rr * HR * ur;
+    }
+}
+
+// roeFlux1D2 (fluxSchemes.hpp:13-71)
+CFD_HD void roe_1d(const double *L, const double *R, double *res)
+{
+    const double gamma = kGamma;
+    double rl = L[0], ul = L[1], pl = L[2], rr = R[0], ur = R[1], pr = R[2];
+    double HL = pl / rl * kGamma / (kGamma - 1) + (ul * ul) / 2;
+    double HR = pr / rr * kGamma / (kGamma - 1) + (ur * ur) / 2;
+    double srl = sqrt(rl), srr = sqrt(rr);
+    double rBar = sqrt(rl * rr);
+    double uBar = (ul * srl + ur * srr) / (srl + srr);
+    double HBar = (HL * srl + HR * srr) / (srl + srr);
+    double cBar = sqrt((gamma - 1) * (HBar - uBar * uBar / 2));
+    double cBar2 = (gamma - 1) * (HBar - uBar * uBar / 2);
+    double dr = rr - rl, du = ur - ul, dp = pr - pl;
+    double lambda[3] = {fabs(uBar), fabs(uBar + cBar), fabs(uBar - cBar)};
+    double eps = 0.1 * (fabs(uBar) + cBar);
+    for (int i = 0; i < 3; i++)
+        if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) / (2.0 * eps);
+    double a0 = lambda[0] * (dr - dp / cBar2);
+    double a1 = lambda[1] / (2.0 * cBar2) * (dp + rBar * cBar * du);
+    double a2 = lambda[2] / (2.0 * cBar2) * (dp - rBar * cBar * du);
+    double a3 = a0 + a1 + a2;
+    double a4 = cBar * (a1 - a2);
+    double FL[3] = {rl * ul, rl * ul * ul + pl, rl * HL * ul};
+    double FR[3] = {rr * ur, rr * ur * ur + pr, rr * HR * ur};
+    for (int i = 0; i < 3; i++) res[i] = (FL[i] + FR[i]) / 2.0;
+    res[0] -= 0.5 * a3;
+    res[1] -= 0.5 * (a3 * uBar + a4);
+    res[2] -= 0.5 * (HBar * a3 + uBar * a4 - cBar2 * a0 / (gamma - 1));
+}
+
+// HLLCFlux2D2 (fluxSchemes.hpp:202-327); the 3D form treats the two
+// tangential momentum components alike.
+template <int NV, int AX>
+CFD_HD void hllc_md(const double *L, const double *R, double *res)
+{
+    constexpr int D = NV - 2, E = NV - 1;
+    const double gamma = kGamma;
+    const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+    double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
+    const double *vl = L + 1, *vr = R + 1;
+    double HL, HR;
+    if constexpr (D == 2) {
+        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
+    } else {
+        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
+    }
+    double VnL = vl[AX], VnR = vr[AX];
+    double cl = sqrt(pl / rl * gamma), cr = sqrt(pr / rr * gamma);
+    double rBar = (rl + rr) / 2, cBar = (cl + cr) / 2;
+    double ps0 = (pl + pr) / 2 - rBar * cBar * (VnR - VnL) / 2;
+    double ps = (0.0 < ps0) ? ps0 : 0.0;  // std::max(0.0, .)
+    double ql = (ps <= pl) ? 1.0 : sqrt(1.0 + (gamma + 1.0) / (2.0 * gamma) * (ps / pl - 1.0));
+    double qr = (ps <= pr) ? 1.0 : sqrt(1.0 + (gamma + 1.0) / (2.0 * gamma) * (ps / pr - 1.0));
+    double SL = VnL - cl * ql, SR = VnR + cr * qr;
+    double Sstar = ((pr - pl) + (rl * VnL * (SL - VnL) - rr * VnR * (SR - VnR))) / (rl * (SL - VnL) - rr * (SR - VnR));
+
+    // Physical flux F and star-state difference for one side
+    // (the reference spells the tangential selector as u*norm[1] / v*norm[0];
+    // for unit axis normals that is u_i * (1 - n_i)).
+    auto side_flux = [&](double r, const double *v, double p, double H, double Vn, double S, double *out, double scale,
+                         bool accumulate) {
+        double U[NV], F[NV], Ustar[NV];
+        U[0] = r;
+        for (int i = 0; i < D; i++) U[1 + i] = r * v[i];
+        U[E] = r * H - p;
+        F[0] = r * Vn;
+        for (int i = 0; i < D; i++) F[1 + i] = r * v[i] * Vn + p * n[i];
+        F[E] = r * H * Vn;
+        double Usf = (S - Vn) / (S - Sstar);
+        Ustar[0] = Usf * r;
+        for (int i = 0; i < D; i++) Ustar[1 + i] = Usf * (Sstar * n[i] + v[i] * (1.0 - n[i])) * r;
+        Ustar[E] = Usf * (U[E] + (Sstar - Vn) * (r * Sstar + p / (S - Vn)));
+        for (int i = 0; i < NV; i++) {
+            double f = F[i] + S * (Ustar[i] - U[i]);
+            if (scale != 1.0) f = f / 2;
+            if (accumulate) out[i] += f; else out[i] = f;
+        }
+    };
+    if (SL > 0) {
+        res[0] = rl * VnL;
+        for (int i = 0; i < D; i++) res[1 + i] = rl * vl[i] * VnL + pl * n[i];
+        res[E] = rl * HL * VnL;
+    } else if (Sstar > 0) {
+        side_flux(rl, vl, pl, HL, VnL, SL, res, 1.0, false);
+    } else if (Sstar == 0) {
+        side_flux(rl, vl, pl, HL, VnL, SL, res, 0.5, false);
+        side_flux(rr, vr, pr, HR, VnR, SR, res, 0.5, true);
+    } else if (SR > 0) {
+        side_flux(rr, vr, pr, HR, VnR, SR, res, 1.0, false);
+    } else {
+        res[0] = rr * VnR;
+        for (int i = 0; i < D; i++) res[1 + i] = rr * vr[i] * VnR + pr * n[i];
+        res[E] = rr * HR * VnR;
+    }
+}
+
+// roeFlux2DSym (fluxSchemes.hpp:420-553), 3D form with both tangential
+// components in the linear wave.
+template <int NV, int AX>
+CFD_HD void roe_md(const double *L, const double *R, double *res)
+{
+    constexpr int D = NV - 2, E = NV - 1;
+    const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+    double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
+    const double *vl = L + 1, *vr = R + 1;
+    double HL, HR;
+    if constexpr (D == 2) {
+        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
+    } else {
+        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
+    }
+    double VnL = vl[AX], VnR = vr[AX];
+    double FcL[NV], FcR[NV];
+    FcL[0] = rl * VnL;
+    for (int i = 0; i < D; i++) FcL[1 + i] = rl * vl[i] * VnL + pl * n[i];
+    FcL[E] = rl * HL * VnL;
+    FcR[0] = rr * VnR;
+    for (int i = 0; i < D; i++) FcR[1 + i] = rr * vr[i] * VnR + pr * n[i];
+    FcR[E] = rr * HR * VnR;
+
+    double coef1 = sqrt(rl), coef2 = sqrt(rr);
+    double divisor = 1.0 / (coef1 + coef2);
+    double rhoAvg = sqrt(rl * rr);
+    double vAvg[3];
+    for (int i = 0; i < D; i++) vAvg[i] = (coef1 * vl[i] + coef2 * vr[i]) * divisor;
+    double HAvg = (coef1 * HL + coef2 * HR) * divisor;
+    double q_2Avg;
+    if constexpr (D == 2) q_2Avg = (vAvg[0] * vAvg[0] + vAvg[1] * vAvg[1]) / 2;
+    else q_2Avg = (vAvg[0] * vAvg[0] + vAvg[1] * vAvg[1] + vAvg[2] * vAvg[2]) / 2;
+    double cAvg = sqrt((kGamma - 1) * (HAvg - q_2Avg));
+    double VnAvg = vAvg[AX];
+    double lambda[3] = {fabs(VnAvg - cAvg), fabs(VnAvg), fabs(VnAvg + cAvg)};
+    double eps = 0.05 * (fabs(VnAvg) + cAvg);
+    for (int i = 0; i < 3; i++)
+        if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) / (2.0 * eps);
+
+    double deltaP = pr - pl, deltaVn = VnR - VnL, deltaRho = rr - rl;
+    double dv[3];
+    for (int i = 0; i < D; i++) dv[i] = vr[i] - vl[i];
+    double Fd[NV];
+    double c1 = (deltaP - rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+    Fd[0] = lambda[0] * (c1 * 1);
+    for (int i = 0; i < D; i++) Fd[1 + i] = lambda[0] * (c1 * (vAvg[i] - cAvg * n[i]));
+    Fd[E] = lambda[0] * (c1 * (HAvg - cAvg * VnAvg));
+
+    double cc = (deltaP + rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+    Fd[0] += lambda[2] * (cc * 1);
+    for (int i = 0; i < D; i++) Fd[1 + i] += lambda[2] * (cc * (vAvg[i] + cAvg * n[i]));
+    Fd[E] += lambda[2] * (cc * (HAvg + cAvg * VnAvg));
+
+    double c2 = deltaRho - deltaP / (cAvg * cAvg);
+    Fd[0] += lambda[1] * (c2 * 1.0 + rhoAvg * 0.0);
+    // tangential components carry rhoAvg * dv_i, the normal one 0
+    // (fluxSchemes.hpp:526-528 for axis normals).
+    double tE = 0.0;
+    bool first = true;
+    for (int i = 0; i < D; i++) {
+        double ti = (i == AX) ? 0 : dv[i];
+        Fd[1 + i] += lambda[1] * (c2 * vAvg[i] + rhoAvg * ti);
+        if (i != AX) {
+            double term = vAvg[i] * dv[i];
+            if (first) { tE = term; first = false; } else tE = tE + term;
+        }
+    }
+    Fd[E] += lambda[1] * (c2 * q_2Avg + rhoAvg * tE);
+    for (int i = 0; i < NV; i++) res[i] = (FcL[i] + FcR[i] - Fd[i]) / 2;
+}
+
+template <int NV, int AX, int FLUX>
+CFD_HD void riemann(const double *L, const double *R, double *res)
+{
+    if constexpr (NV == 3) {
+        if constexpr (FLUX == FLUX_HLLC) hllc_1d(L, R, res); else roe_1d(L, R, res);
+    } else {
+        if constexpr (FLUX == FLUX_HLLC) hllc_md<NV, AX>(L, R, res); else roe_md<NV, AX>(L, R, res);
+    }
+}
+
+// Physical (node) flux: fluxSolveEuler1D / fluxSolveEuler2D
+// (fluxSchemes.hpp:572-599); the 3D form adds w.
+template <int NV, int AX>
+CFD_HD void node_flux(const double *p, double *f)
+{
+    if constexpr (NV == 3) {
+        double r = p[0], u = p[1], pp = p[2];
+        f[0] = r * u;
+        f[1] = r * u * u + pp;
+        f[2] = (kGamma / (kGamma - 1) * pp + r * (u * u) / 2) * u;
+    } else {
+        constexpr int D = NV - 2, E = NV - 1;
+        const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+        double r = p[0], pp = p[E];
+        double Vn;
+        if constexpr (D == 2) Vn = (p[1] * n[0] + p[2] * n[1]);
+        else Vn = (p[1] * n[0] + p[2] * n[1] + p[3] * n[2]);
+        f[0] = r * Vn;
+        for (int i = 0; i < D; i++) f[1 + i] = r * p[1 + i] * Vn + n[i] * pp;
+        double q2;
+        if constexpr (D == 2) q2 = (p[1] * p[1] + p[2] * p[2]);
+        else q2 = (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+        f[E] = (q2 / 2 * r + kGamma / (kGamma - 1) * pp) * Vn;
+    }
+}
+
+// MidNodeAndNodeDif6 (differ.cpp:54-103): one cell's contribution,
+// (w1 (Fn[i+1]-Fn[i-1]) + w0 (Fh[i+1/2]-Fh[i-1/2]) + w2 (Fh[i+3/2]-Fh[i-3/2])) / h.
+CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fhp1, double fhp3, double h)
+{
+    const double w0 = 3.0 / 2.0, w1 = -3.0 / 10.0, w2 = 1.0 / 30.0;
+    return (w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3)) / h;
+}
+
+} // namespace cfd

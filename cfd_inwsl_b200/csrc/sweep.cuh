@@ -1,0 +1,315 @@
+// Fused per-direction line sweep of the zone_FD right-hand side.
+//
+// Replaces SpDistributor::rhsSolve (zone_FD/src/src/sp_distributor.cpp:3-79)
+// for one direction together with Equation::consToPrim (equation.cpp:8-93)
+// and OneDBnd::update (oneDBnd.cpp:31-114) for the lines it touches, and
+// optionally the RK3 stage combination of BlockSolver::RK3_SSP
+// (blockSolver.cpp:58-86) plus the reductions for the log value and the next
+// CFL step.
+//
+// Work decomposition. A CTA owns W neighbouring lines along the sweep axis AX
+// and one segment [s_begin, s_end) of them. It marches through the segment in
+// chunks of S cells. Per chunk it
+//   1. loads the S new cells (cons -> prim on the fly, ghost cells from the
+//      line's boundary wiring) into a shared-memory ring of S+8 positions,
+//   2. computes the S new face fluxes (one face per thread) into a ring of
+//      S+3 faces; the 3 faces shared with the previous chunk are reused,
+//   3. applies the MND6 difference (node fluxes recomputed from the prim ring)
+//      and the epilogue for S cells.
+// Face values and face fluxes never leave shared memory, and every cell is
+// read from HBM once per sweep plus 8 halo cells per line segment.
+//
+// Thread layout: along x (AX = 0) consecutive threads take consecutive cells
+// of a line; along y/z consecutive threads take neighbouring lines (adjacent
+// x), so every global access is coalesced along x in all three sweeps.
+#pragma once
+#include "euler_math.cuh"
+#include "sweep_params.h"
+
+namespace cfd {
+namespace CFD_NS {
+
+template <int NV>
+__device__ __forceinline__ void load_cons_prim(const double *__restrict__ u, long long ncell, long long cell,
+                                               double *pr)
+{
+    double c[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) c[v] = __ldg(u + v * ncell + cell);
+    cons_to_prim<NV>(c, pr);
+}
+
+// Ghost cell k (0 = nearest the boundary) of a line end, as OneDBnd::update
+// leaves it after Bnds::update (oneDBnd.cpp:31-114).
+template <int NV>
+__device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &bl, int k, double *pr)
+{
+    switch (bl.type) {
+    case BND_PERIODIC1D:
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0 + (long long)k * bl.offset, pr);
+        return;
+    case BND_SUPERSONICOUTLET:
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0, pr);
+        return;
+    case BND_SYMMETRYX:
+    case BND_SYMMETRYY:
+    case BND_SYMMETRYZ:
+    case BND_SYMMETRY1D: {
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0 + (long long)k * bl.offset, pr);
+        int neg = (bl.type == BND_SYMMETRYY) ? 2 : (bl.type == BND_SYMMETRYZ) ? 3 : 1;
+        if (neg < NV - 1) pr[neg] = -pr[neg];
+        if (bl.type == BND_SYMMETRY1D) {
+            // SYMMETRY1D writes only the first three values of each ghost cell.
+            for (int v = 3; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * 4 + k) * NV + v] : 0.0;
+        }
+        return;
+    }
+    case BND_DOUBLEMACHUP: {
+        // oneDBnd.cpp:87-108: exact post- or pre-shock state at the stage time.
+        // As in the reference, ghost k is placed at y = -dh/2 + k*dh (measured
+        // from 0, not from the line end) and x is the edge cell's centre.
+        double x = bl.coor_x;
+        double y = -bl.dh_y / 2 + k * bl.dh_y;
+        double gt = 1.0 / 6.0 + sqrt(3.0) / 3.0 * (1.0 + 20 * p.t);
+        if (y > sqrt(3.0) * (x - gt)) {
+            pr[0] = 8.0; pr[1] = p.dm_u; pr[2] = p.dm_v; pr[NV - 1] = 116.5;
+        } else {
+            pr[0] = 1.4; pr[1] = 0; pr[2] = 0; pr[NV - 1] = 1.0;
+        }
+        if (NV == 5) pr[3] = 0.0;
+        return;
+    }
+    default:
+        // DIRICLET and every type whose update() is a no-op keep their static data.
+        for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * 4 + k) * NV + v] : 0.0;
+        return;
+    }
+}
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W>
+struct SweepShape {
+    static constexpr int NT = S * W;
+    static constexpr int R = S + 8;           // prim ring positions
+    static constexpr int RF = S + 3;          // face ring positions
+    static constexpr int LSP = R | 1;         // odd line strides avoid bank conflicts
+    static constexpr int LSF = RF | 1;
+    static constexpr int SMEM_DOUBLES = 2 * NV * W * LSP + NV * W * LSF;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+};
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W>
+__global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(const SweepParams p)
+{
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
+    extern __shared__ double smem[];
+    double *sp = smem;                   // [NV][W][LSP] prim
+    double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue)
+    double *sf = sc + NV * W * LSP;      // [NV][W][LSF] face flux
+
+    constexpr int T0 = (AX == 0) ? 1 : 0;  // transverse axis with neighbouring lines in a CTA
+    constexpr int T1 = (AX == 2) ? 1 : 2;
+    const int nd = p.n[AX];
+    const int nt0 = p.n[T0];
+    const int nseg = (nd + p.seg_len - 1) / p.seg_len;
+    const int nblk0 = (nt0 + W - 1) / W;
+    int bid = blockIdx.x;
+    const int seg = bid % nseg;
+    bid /= nseg;
+    const int a0 = (bid % nblk0) * W;
+    const int bb = bid / nblk0;
+    const int s_begin = seg * p.seg_len;
+    const int s_end = min(s_begin + p.seg_len, nd);
+
+    const int tid = threadIdx.x;
+    const int tl = (AX == 0) ? tid / S : tid % W;   // line within the CTA
+    const int tp = (AX == 0) ? tid % S : tid / W;   // position within the chunk
+    const long long sAX = p.stride[AX];
+
+    auto line_of = [&](int l, bool &ok, long long &base, int &lid) {
+        int a = a0 + l;
+        ok = a < nt0;
+        base = (long long)a * p.stride[T0] + (long long)bb * p.stride[T1];
+        lid = a + nt0 * bb;
+    };
+
+    // Stage cell P (global index along AX, may be a ghost) of line l.
+    auto load_pos = [&](int l, int P) {
+        bool ok; long long base; int lid;
+        line_of(l, ok, base, lid);
+        double pr[NV];
+        if (!ok) {
+            pr[0] = 1.0;
+            for (int v = 1; v < NV - 1; v++) pr[v] = 0.0;
+            pr[NV - 1] = 1.0;
+        } else if (P >= 0 && P < nd) {
+            load_cons_prim<NV>(p.u, p.ncell, base + (long long)P * sAX, pr);
+        } else if (P < 0) {
+            int k = -P - 1;
+            ghost_prim<NV>(p, p.bc_lo[lid], k > 3 ? 3 : k, pr);
+        } else {
+            int k = P - nd;
+            ghost_prim<NV>(p, p.bc_hi[lid], k > 3 ? 3 : k, pr);
+        }
+        double cs[NV];
+        prim_to_cons<NV>(pr, cs);
+        int slot = (P - s_begin + 4) % R;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            sp[(v * W + l) * LSP + slot] = pr[v];
+            sc[(v * W + l) * LSP + slot] = cs[v];
+        }
+    };
+
+    // Face j lies between cells j-1 and j (x_{j-1/2}); stencil cells j-3..j+2.
+    auto face = [&](int l, int j) {
+        double pr6[6][NV], cs6[6][NV];
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            int slot = (j - 3 + m - s_begin + 4) % R;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                pr6[m][v] = sp[(v * W + l) * LSP + slot];
+                cs6[m][v] = sc[(v * W + l) * LSP + slot];
+            }
+        }
+        double fl[NV], fr[NV], fx[NV];
+        reconstruct_face<NV, AX, FAM>(pr6, cs6, p.icst, fl, fr);
+        riemann<NV, AX, FLUX>(fl, fr, fx);
+        int fslot = (j - s_begin + 1) % RF;
+#pragma unroll
+        for (int v = 0; v < NV; v++) sf[(v * W + l) * LSF + fslot] = fx[v];
+    };
+
+    // prologue: cells s_begin-4 .. s_begin+3
+    for (int idx = tid; idx < 8 * W; idx += NT) {
+        int l = (AX == 0) ? idx / 8 : idx % W;
+        int q = (AX == 0) ? idx % 8 : idx / W;
+        load_pos(l, s_begin - 4 + q);
+    }
+
+    double red_rho = 0.0, red_lam[3] = {0.0, 0.0, 0.0};
+    unsigned err = 0;
+
+    for (int c0 = s_begin; c0 < s_end; c0 += S) {
+        load_pos(tl, c0 + 4 + tp);
+        __syncthreads();
+        if (c0 == s_begin) {
+            for (int idx = tid; idx < 3 * W; idx += NT) {
+                int l = (AX == 0) ? idx / 3 : idx % W;
+                int q = (AX == 0) ? idx % 3 : idx / W;
+                face(l, s_begin - 1 + q);
+            }
+        }
+        face(tl, c0 + 2 + tp);
+        __syncthreads();
+
+        const int i = c0 + tp;
+        bool ok; long long base; int lid;
+        line_of(tl, ok, base, lid);
+        if (ok && i < s_end) {
+            double pm[NV], pp[NV], fnm[NV], fnp[NV];
+            int sm = (i - 1 - s_begin + 4) % R, spp = (i + 1 - s_begin + 4) % R;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                pm[v] = sp[(v * W + tl) * LSP + sm];
+                pp[v] = sp[(v * W + tl) * LSP + spp];
+            }
+            node_flux<NV, AX>(pm, fnm);
+            node_flux<NV, AX>(pp, fnp);
+            int f0 = (i - 1 - s_begin + 1) % RF, f1 = (i - s_begin + 1) % RF, f2 = (i + 1 - s_begin + 1) % RF,
+                f3 = (i + 2 - s_begin + 1) % RF;
+            const long long cell = base + (long long)i * sAX;
+            double uo[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const double *fv = sf + (v * W + tl) * LSF;
+                double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h);
+                const long long gi = v * p.ncell + cell;
+                double r = p.first ? (0.0 + d) : (p.rhs[gi] + d);
+                if (p.mode != MODE_RK) {
+                    p.rhs[gi] = r;
+                } else {
+                    if (v == 0 && p.want_reduce) red_rho = fmax(red_rho, fabs(r));
+                    double o;
+                    if (p.rk_stage == 1) {
+                        o = p.u0[gi] - p.rkBdt * r;
+                    } else {
+                        o = p.rkA * p.u0[gi] - p.rkBdt * r + p.rkC * p.u[gi];
+                    }
+                    uo[v] = o;
+                    p.u_out[gi] = o;
+                }
+            }
+            if (p.mode == MODE_RK) {
+                bool fin = true;
+#pragma unroll
+                for (int v = 0; v < NV; v++) fin = fin && isfinite(uo[v]);
+                if (!fin) err |= ERR_NONFINITE;
+                if (p.want_reduce) {
+                    double pr[NV];
+                    cons_to_prim<NV>(uo, pr);
+                    if (!(pr[0] > 0.0) || !(pr[NV - 1] > 0.0)) err |= ERR_NEGATIVE;
+                    double cs = sqrt(kGamma * pr[NV - 1] / pr[0]);
+#pragma unroll
+                    for (int d = 0; d < NV - 2; d++) red_lam[d] = fmax(red_lam[d], (cs + fabs(pr[1 + d])) / p.hdir[d]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (p.mode == MODE_RK) {
+        if (err) atomicOr(p.err, err);
+        if (p.want_reduce) block_max_reduce<NT, 4>(red_rho, red_lam, p.red);
+    }
+}
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W>
+static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
+{
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    constexpr int T0 = (AX == 0) ? 1 : 0;
+    constexpr int T1 = (AX == 2) ? 1 : 2;
+    long long nseg = (p.n[AX] + p.seg_len - 1) / p.seg_len;
+    long long nblk = (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
+    if (nblk <= 0) return cudaSuccess;
+    if (nblk > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    sweep_kernel<NV, AX, FAM, FLUX, S, W><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
+    return cudaGetLastError();
+}
+
+// Tile shapes: along x, 64 cells x 4 lines; along y/z, 8 cells x 32 lines
+// (1D: 128 cells of one line).
+template <int NV, int FAM>
+cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st)
+{
+    if constexpr (NV == 3) {
+        if (ax != 0) return cudaErrorInvalidValue;
+        return flux == FLUX_HLLC ? launch_sweep_shape<3, 0, FAM, FLUX_HLLC, 128, 1>(p, st)
+                                 : launch_sweep_shape<3, 0, FAM, FLUX_ROE, 128, 1>(p, st);
+    } else {
+        if (ax == 0)
+            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, 64, 4>(p, st)
+                                     : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, 64, 4>(p, st);
+        if (ax == 1)
+            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 1, FAM, FLUX_HLLC, 8, 32>(p, st)
+                                     : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, 8, 32>(p, st);
+        if constexpr (NV == 5) {
+            if (ax == 2)
+                return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, 8, 32>(p, st)
+                                         : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, 8, 32>(p, st);
+        }
+        return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace CFD_NS
+} // namespace cfd

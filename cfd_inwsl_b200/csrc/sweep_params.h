@@ -1,0 +1,89 @@
+// Parameter blocks shared by the sweep kernels and the host launcher.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace cfd {
+
+// BndType values (zone_FD/src/include/macro.hpp:33-34) plus the 3D mirror.
+enum : int {
+    BND_TYPENULL = 0,
+    BND_PERIODIC1D = 1,
+    BND_SYMMETRY1D = 2,
+    BND_DIRICLET = 3,
+    BND_SUPERSONICOUTLET = 7,
+    BND_DOUBLEMACHUP = 8,
+    BND_SYMMETRYX = 10,
+    BND_SYMMETRYY = 11,
+    BND_SYMMETRYZ = 12,
+};
+
+// One line end's ghost wiring, the device image of a OneDBnd
+// (zone_FD/src/include/oneDBnd.hpp:10-33): source cell i0 and stride offset
+// for the copying types, a slot in the static ghost-value table for the
+// others, and the coordinates DoubleMachUp evaluates its exact state at.
+struct BcLine {
+    long long i0;
+    int offset;
+    int type;
+    int slot;      // -1: no static data (zeros)
+    int pad;
+    double coor_x; // DoubleMachUp: x of the line's edge cell centre
+    double dh_y;   // DoubleMachUp: edge cell centre minus its inner neighbour, y
+};
+
+enum SweepMode : int { MODE_WRITE = 0, MODE_RK = 2 };
+enum ErrBits : unsigned { ERR_NONFINITE = 1u, ERR_NEGATIVE = 2u, ERR_TIMEOUT = 4u };
+
+struct SweepParams {
+    const double *u;    // current state U_k, planar SoA u[v * ncell + cell]
+    const double *u0;   // RK base state U_0
+    double *rhs;        // running right-hand side (SoA)
+    double *u_out;      // RK stage output (SoA); never aliases u
+    long long ncell;
+    int n[3];
+    long long stride[3];
+    double h;           // spacing used by the difference along this axis (Info::geth)
+    double hdir[3];     // spacings for the wave-speed reduction
+    int mode;           // MODE_WRITE: rhs = prev + D ; MODE_RK: stage combination
+    int first;          // 1: this is the first sweep of the stage (prev = 0)
+    int rk_stage;       // 1, 2, 3
+    double rkA, rkBdt, rkC;  // U_out = (A U0 - Bdt R) + C U_k   (stage 1: U0 - dt R)
+    int want_reduce;    // 1: max |R_rho| and per-direction max wave speed of U_out
+    unsigned long long *red;  // [0] max |R_rho| bits, [1..3] wave-speed maxima bits
+    unsigned *err;      // ErrBits
+    const BcLine *bc_lo;  // per line (index a + n[T0] * b), low end
+    const BcLine *bc_hi;  // per line, high end
+    const double *bc_vals; // static ghost prim values [slot][4][NV]
+    double t;           // stage time
+    double dm_u, dm_v;  // DoubleMachUp post-shock velocity, 8.25 cos(pi/6) and -8.25 sin(pi/6) from the host libm
+    double icst;        // interpolator constant (TENO cutoff)
+    int seg_len;        // cells per CTA segment along the sweep
+};
+
+// Block-wide max of non-negative doubles followed by one atomicMax per value.
+// NaN inputs are ignored (fmax), like the reference's comparisons that never
+// let a NaN replace the running maximum.
+template <int NT, int NRED>
+__device__ __forceinline__ void block_max_reduce(double v0, const double *v123, unsigned long long *out)
+{
+    __shared__ double red_s[NRED][NT / 32];
+    double v[NRED];
+    v[0] = v0;
+    for (int k = 1; k < NRED; k++) v[k] = v123[k - 1];
+    for (int k = 0; k < NRED; k++) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        v[k] = x;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < NRED; k++) red_s[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x < NRED) {
+        double x = 0.0;
+        for (int w = 0; w < NT / 32; w++) x = fmax(x, red_s[threadIdx.x][w]);
+        if (x > 0.0) atomicMax(out + threadIdx.x, (unsigned long long)__double_as_longlong(x));
+    }
+}
+
+} // namespace cfd

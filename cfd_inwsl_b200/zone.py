@@ -1,0 +1,366 @@
+"""Python mirror of the zone_FD solver interface over the GPU library.
+
+Names follow the reference so that code written against it reads the same:
+
+  * ``InterMethod``, ``FluxMethod``, ``DiffMethod``, ``BndType``, ``EquationType``
+    mirror the enums of zone_FD/src/include/macro.hpp:33-90 (same values);
+  * ``Info`` mirrors zone_FD/src/include/info.hpp (fields, ``icMax``, ``geth``,
+    ``nPrim``, ``nGhostCell``);
+  * ``BlockSolver`` mirrors zone_FD/src/include/blockSolver.hpp: ``solve``,
+    ``RK3_SSP``, ``getTimeIntervalExplicit``, ``stepsLoopCFL``, ``timesteps``,
+    with the state in the reference's AoS ``Data`` layout (``cons``/``prim``/``rhs``
+    numpy arrays of shape (ncell, nvar)).
+
+The boundary wiring follows Initializer::initBnds (initializer.cpp:743-870)
+for the Euler cases; initial states are supplied by the caller (``set_cons``)
+or by :func:`sod_1d` for the Sod case of Initializer::solInit
+(initializer.cpp:87-109). Every computation runs in libcfdgpu.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import math
+
+import numpy as np
+
+from . import _lib
+
+
+class BndType(enum.IntEnum):  # macro.hpp:33-34
+    TYPENULL = 0
+    PERIODIC1D = 1
+    SYMMETRY1D = 2
+    DIRICLET = 3
+    DIRICLET_SODL = 4
+    DIRICLET_SODR = 5
+    FLUXGHOST = 6
+    SUPERSONICOUTLET = 7
+    DoubleMachUp = 8
+    ARDBND = 9
+    SYMMETRYX = 10
+    SYMMETRYY = 11
+    SYMMETRYZ = 12          # extension: 3D mirror in z
+    PERIODIC_WRAP = 100     # extension: PERIODIC1D wired as a true wrap
+
+
+class InterMethod(enum.IntEnum):  # macro.hpp:37-78
+    FIRSTORDER = 0
+    MUSCL = 1
+    WCNS5 = 2
+    WCNSZ5 = 3
+    WCNS5Char = 4
+    WCNSZ5Char = 5
+    WCNS5CONG = 6
+    TCNSCongA = 7
+    WCNS5CONGZ = 8
+    WCNS5CONGZCT4 = 9
+    WCNS5CONGZCT7 = 10
+    TCNS5 = 11
+    TCNS5CT4 = 12
+    TCNS5CT7 = 13
+    LINEAR5 = 14
+    MUCSLIN5 = 15
+    INTERMAX = 16
+    whfTCNSN = 17
+    whfTCNSNA = 18
+    whfTCNSNAS = 19
+    whfTCNSNS = 20
+    whfTCNSNLAD = 21
+    congTCNS5CT5 = 22
+    congTCNS5CT10 = 23
+    whfAITCNSNS = 24
+    whfAITCNSNA = 25
+    whfAITCNSNAS_1 = 26
+    whfAITCNSNAS_2 = 27
+    whfAITCNSNLADS = 28
+    whfAITCNSNAZS = 29
+    whfAITCNSNmyASF002_1 = 30
+    whfAITCNSNmyASF002_2 = 31
+    whfAITCNSNmyASF002_ai1 = 32
+    whfzycTCNSNmyASF002_1 = 33
+    whfCOMPARE = 34
+    new_TCNS5 = 35
+    new_WHFTCNSA = 36
+    new_WCNS5CONGZ = 37
+    new_WHFTCNSASF203_NoS = 38
+    new_WHFTCNSASF202_NoS = 39
+
+
+class DiffMethod(enum.IntEnum):  # macro.hpp:82
+    HDS6 = 0
+    TRAD6 = 1
+    TRAD2 = 2
+    MND6 = 3
+
+
+class EquationType(enum.IntEnum):  # macro.hpp:84
+    LINEARCONV1D = 0
+    BURGERS1D = 1
+    EULER = 2
+    ACCURACYTEST = 3
+
+
+class FluxMethod(enum.IntEnum):  # macro.hpp:86
+    HLLC = 0
+    ROE = 1
+
+
+GAMMA = 1.4  # macro.hpp:28
+
+
+class Info:
+    """Mirror of the reference's Info (info.hpp:4-66) with its defaults."""
+
+    def __init__(self):
+        self.spMethod = InterMethod.WCNS5
+        self.eqType = EquationType.EULER
+        self.nCase = 2
+        self.t = 0.0
+        self.dt = 0.0001
+        self.step = 0
+        self.endStep = 25000
+        self.outputInterval = 100
+        self.outputDt = 0.01
+        self.outputT = 0.0
+        self.CFL = 0.5
+        self.diffMethod = DiffMethod.MND6
+        self.interMethod = InterMethod.WCNS5
+        self.fluxMethod = FluxMethod.ROE
+        self.iMax = [201, 201, 2]
+        self.calZone = [0.0, 0.3, 0.0, 0.3, 0.0, 2.0]
+        self.constH = True
+        self.dim = self.getDim()
+        # GPU-only knobs (no counterpart in the reference)
+        self.strict = False     # bitwise-parity build of the kernels
+        self.device = 0
+        self.seg_len = [0, 0, 0]
+
+    def getDim(self) -> int:  # info.cpp:103-114
+        return sum(1 for i in range(3) if self.iMax[i] > 2)
+
+    def icMax(self) -> list[int]:  # info.cpp:117-129
+        return [1 if self.iMax[i] < 2 else self.iMax[i] - 1 for i in range(3)]
+
+    def geth(self, idim: int) -> float:  # info.cpp:359-365 with constH (initializer.cpp:604-609)
+        if self.constH:
+            return (self.calZone[1] - self.calZone[0]) / (self.iMax[0] - 1)
+        return (self.calZone[2 * idim + 1] - self.calZone[2 * idim]) / (self.iMax[idim] - 1)
+
+    def nPrim(self) -> int:
+        return {1: 3, 2: 4, 3: 5}[self.dim]
+
+    nCons = nPrim
+
+    def nGhostCell(self) -> int:  # info.cpp:7-22 (WCNS5 + MND6)
+        return 4
+
+
+def default_bc_types(info: Info) -> list[list[int]]:
+    """Per direction/side BndType of Initializer::initBnds for Euler
+    (initializer.cpp:775-811): outlets by default, mirrors for nCase 2,
+    SYMMETRYX/DIRICLET for nCase 3 (RTI), PERIODIC1D for nCase 6."""
+    bc = [[BndType.SUPERSONICOUTLET] * 2 for _ in range(3)]
+    if info.dim == 1:
+        if info.nCase == 4:
+            bc[0] = [BndType.SYMMETRY1D] * 2
+    else:
+        if info.nCase == 2:
+            bc[0] = [BndType.SYMMETRYX] * 2
+            bc[1] = [BndType.SYMMETRYY] * 2
+        elif info.nCase == 3:
+            bc[0] = [BndType.SYMMETRYX] * 2
+            bc[1] = [BndType.DIRICLET] * 2
+        elif info.nCase == 6:
+            bc = [[BndType.PERIODIC1D] * 2 for _ in range(3)]
+    return bc
+
+
+class BlockSolver:
+    """GPU counterpart of BlockSolver (blockSolver.hpp:7-57) for the Euler path.
+
+    ``bc`` overrides the per-direction boundary types ([[lo, hi], ...]);
+    ``periodic=True`` wires every direction as a true periodic wrap.
+    """
+
+    def __init__(self, info: Info, bc=None, periodic: bool = False):
+        self.info = info
+        self.lib = _lib.load()
+        self.dim = info.dim
+        self.nvar = info.nPrim()
+        self.n = info.icMax()
+        self.ncell = self.n[0] * self.n[1] * self.n[2]
+        self.timesteps = 0
+        cfg = _lib.CfdConfig()
+        self.lib.cfd_config_default(C.byref(cfg))
+        cfg.dim = info.dim
+        for d in range(3):
+            cfg.n[d] = self.n[d] if d < info.dim else 1
+            cfg.h[d] = info.geth(d)
+            cfg.x0[d] = info.calZone[2 * d]
+            cfg.seg_len[d] = int(info.seg_len[d])
+        cfg.inter_method = int(info.interMethod)
+        cfg.flux_method = int(info.fluxMethod)
+        cfg.diff_method = int(info.diffMethod)
+        cfg.strict = int(bool(info.strict))
+        cfg.device = int(info.device)
+        types = bc if bc is not None else default_bc_types(info)
+        if periodic:
+            types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]
+        for d in range(3):
+            for s in range(2):
+                cfg.bc[d][s] = int(types[d][s])
+        self.cfg = cfg
+        h = C.c_void_p()
+        rc = self.lib.cfd_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise _lib.CfdError(rc, "cfd_create")
+        self.h = h
+        if info.dim == 2 and info.nCase == 3 and bc is None and not periodic:
+            self._wire_rti()
+
+    # --- lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- boundary wiring
+    def set_line_bc(self, idim: int, i: int, j: int, side: int, bnd_type: int, i0: int = 0, offset: int = 0,
+                    ghost_prim=None):
+        """Mirror of OneDBnd::setUpdate/setValue for one line end (idim 1-based)."""
+        gp = None
+        if ghost_prim is not None:
+            gp = np.ascontiguousarray(np.broadcast_to(np.asarray(ghost_prim, dtype=np.float64),
+                                                       (4, self.nvar)))
+        _lib.check(self.lib.cfd_set_line_bc(self.h, idim, i, j, side, int(bnd_type), int(i0), int(offset),
+                                            _lib.ptr(gp) if gp is not None else None), self.h)
+
+    def _wire_rti(self):
+        # initializer.cpp:831-861: Dirichlet y ends with (2,0,0,1) below and (1,0,0,2.5) above
+        nx = self.n[0]
+        ny = self.n[1]
+        for i in range(nx):
+            self.set_line_bc(2, i, 0, 0, BndType.DIRICLET, i, nx, [2.0, 0, 0, 1.0])
+            self.set_line_bc(2, i, 0, 1, BndType.DIRICLET, i + (ny - 1) * nx, -nx, [1.0, 0, 0, 2.5])
+
+    # --- state access (reference AoS layout)
+    def set_cons(self, cons: np.ndarray):
+        a = np.ascontiguousarray(cons, dtype=np.float64).reshape(self.ncell, self.nvar)
+        _lib.check(self.lib.cfd_upload_cons(self.h, _lib.ptr(a)), self.h)
+
+    @property
+    def cons(self) -> np.ndarray:
+        out = np.empty((self.ncell, self.nvar))
+        _lib.check(self.lib.cfd_download_cons(self.h, _lib.ptr(out)), self.h)
+        return out
+
+    @property
+    def prim(self) -> np.ndarray:
+        out = np.empty((self.ncell, self.nvar))
+        _lib.check(self.lib.cfd_download_prim(self.h, _lib.ptr(out)), self.h)
+        return out
+
+    def rhsSolve(self) -> np.ndarray:
+        """One RHS evaluation at info.t (RK3_SSP's per-stage body)."""
+        out = np.empty((self.ncell, self.nvar))
+        _lib.check(self.lib.cfd_rhs(self.h, float(self.info.t), _lib.ptr(out)), self.h)
+        return out
+
+    # --- time stepping
+    def getTimeIntervalExplicit(self) -> float:
+        dt = C.c_double()
+        _lib.check(self.lib.cfd_max_dt(self.h, float(self.info.CFL), C.byref(dt)), self.h)
+        return dt.value
+
+    def RK3_SSP(self, dt: float) -> float:
+        """One SSP-RK3 step; returns max |R_rho| of the last stage. Leaves info.t
+        where the reference's RK3_SSP leaves it (t + dt - dt/2 - dt/2)."""
+        linf = C.c_double()
+        _lib.check(self.lib.cfd_rk3_step(self.h, float(dt), float(self.info.t), C.byref(linf)), self.h)
+        self.info.t = ((self.info.t + dt) - dt / 2) - dt / 2
+        return linf.value
+
+    def solve(self, dt: float) -> float:
+        linf = self.RK3_SSP(dt)
+        self.info.t += dt
+        return linf
+
+    def stepsLoopCFL(self, max_steps: int = 1 << 30, record: bool = False):
+        """BlockSolver::stepsLoopCFL (blockSolver.cpp:170-235) without output files:
+        steps until info.step reaches info.endStep. Returns (dts, linfs) if record."""
+        info = self.info
+        eps = 1e-15
+        dts, linfs = [], []
+        k = 0
+        while info.step < info.endStep and k < max_steps:
+            _ = eps
+            dt = self.getTimeIntervalExplicit()
+            if info.outputT + dt > info.outputDt:
+                dt = info.outputDt - info.outputT
+                info.outputT = 0.0
+                info.step += 1
+            else:
+                info.outputT += dt
+            linf = self.solve(dt)
+            self.timesteps += 1
+            k += 1
+            if record:
+                dts.append(dt)
+                linfs.append(linf)
+        return (np.array(dts), np.array(linfs)) if record else None
+
+    def run_device(self, max_steps: int = 1 << 30):
+        """Device-resident stepsLoopCFL (cfd_run): returns (dts, linfs)."""
+        info = self.info
+        t = C.c_double(info.t)
+        ns = C.c_int()
+        cap = min(max_steps, 1 << 22)
+        dts = np.zeros(cap)
+        lin = np.zeros(cap)
+        rc = self.lib.cfd_run(self.h, float(info.CFL), int(info.endStep - info.step), float(info.outputDt), cap,
+                              C.byref(t), C.byref(ns), _lib.ptr(dts), _lib.ptr(lin))
+        _lib.check(rc, self.h)
+        info.t = t.value
+        self.timesteps += ns.value
+        return dts[: ns.value], lin[: ns.value]
+
+
+def sod_1d(info: Info) -> np.ndarray:
+    """Sod initial state of Initializer::solInit (initializer.cpp:87-109):
+    (1, 0, 1) for x < 0, (0.125, 0, 0.1) otherwise, cell centres
+    calZone[0] + (i + 1/2) h. Returns cons (ncell, 3)."""
+    n = info.icMax()[0]
+    h = info.geth(0)
+    out = np.empty((n, 3))
+    gamma = 1.4
+    for i in range(n):
+        x = info.calZone[0] + (i + 0.5) * h
+        if x < 0:
+            out[i] = (1.0, 0.0, 1.0 / (gamma - 1) * 1)
+        else:
+            out[i] = (0.125, 0.0, 1.0 / (gamma - 1) * 0.1)
+    return out
+
+
+def prim_to_cons(prim: np.ndarray) -> np.ndarray:
+    """(rho, u[, v[, w]], p) -> (rho, rho u, ..., rho E) with E = p/(gamma-1)/rho + |u|^2/2."""
+    prim = np.asarray(prim, dtype=np.float64)
+    nv = prim.shape[-1]
+    r = prim[..., 0]
+    vel = prim[..., 1:nv - 1]
+    p = prim[..., nv - 1]
+    out = np.empty_like(prim)
+    out[..., 0] = r
+    out[..., 1:nv - 1] = r[..., None] * vel
+    out[..., nv - 1] = p / (GAMMA - 1) + 0.5 * r * np.sum(vel * vel, axis=-1)
+    return out
+
+
+_ = math

@@ -1,0 +1,162 @@
+/*
+ * cfdgpu.h - C ABI of the B200 (sm_100a) right-hand-side evaluation and
+ * SSP-RK3 time stepper for the zone_FD finite-difference Euler solver.
+ *
+ * The reference evaluates one RK stage inside BlockSolver::RK3_SSP
+ * (zone_FD/src/src/blockSolver.cpp:43-87) as four member calls on host
+ * objects:
+ *     Equation::consToPrim()        equation.cpp:8-29
+ *     Bnds::update()                bnds.cpp:23-27, oneDBnd.cpp:31-114
+ *     SpDistributor::rhsSolve()     sp_distributor.cpp:3-79
+ *     SourceTerm::calSource()       sourceTerm.cpp:50-52 (a no-op without gravity)
+ * followed by an OpenMP stage combination, and computes the CFL step in
+ * BlockSolver::getTimeIntervalExplicit (blockSolver.cpp:318-349). This
+ * library replaces that whole per-stage body with GPU kernels behind the
+ * plain C functions below. No C++ or CUDA types cross the interface.
+ *
+ * Ownership: a handle owns all device memory it allocates. Host pointers are
+ * borrowed for the duration of a call only. Calls on one handle are ordered
+ * on the handle's CUDA stream; a handle is not thread-safe.
+ *
+ * Status: every function returns CFD_OK (0) or a negative CFD_ERR_* code;
+ * cfd_last_error() gives a message for the last failure on a handle. There is
+ * no CPU fallback: if the CUDA kernels cannot run, calls fail.
+ *
+ * Array layout on the host side is the reference's Data layout
+ * (zone_FD/src/src/data.cpp:63): cell-major AoS, data[cell * nvar + var],
+ * cell = i + nx * (j + ny * k), nvar = 3 (1D), 4 (2D) or 5 (3D), conserved
+ * variables (rho, rho*u, rho*v, [rho*w,] rho*E).
+ */
+#ifndef CFDGPU_H
+#define CFDGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define CFD_OK 0
+#define CFD_ERR_CONFIG (-1)          /* invalid configuration or argument */
+#define CFD_ERR_CUDA (-2)            /* a CUDA call failed (message in cfd_last_error) */
+#define CFD_ERR_NONFINITE (-3)       /* a stage produced NaN/Inf in the state */
+#define CFD_ERR_NEGATIVE_STATE (-4)  /* density or pressure <= 0 after a step */
+#define CFD_ERR_TIMEOUT (-5)         /* a bounded device-side wait gave up */
+#define CFD_ERR_UNSUPPORTED (-6)     /* option the library does not implement */
+#define CFD_ERR_NOMEM (-7)           /* device allocation failed */
+
+/* FluxMethod (zone_FD/src/include/macro.hpp:86). */
+#define CFD_FLUX_HLLC 0
+#define CFD_FLUX_ROE 1
+
+/* DiffMethod (macro.hpp:82); only MND6 is implemented. */
+#define CFD_DIFF_MND6 3
+
+/* Arithmetic of the sweep kernels. */
+#define CFD_PREC_FP64 0   /* FP64 everywhere */
+#define CFD_PREC_MIXED 1  /* FP32 reconstruction and face flux, FP64 state/RK/differences */
+
+/* Boundary types: BndType values of macro.hpp:33-34, plus two extensions. */
+#define CFD_BND_TYPENULL 0
+#define CFD_BND_PERIODIC1D 1        /* ghost k = prim(i0 + k*offset) */
+#define CFD_BND_SYMMETRY1D 2        /* mirror, normal (x) velocity negated, 1D */
+#define CFD_BND_DIRICLET 3          /* static ghost values */
+#define CFD_BND_SUPERSONICOUTLET 7  /* ghost k = prim(i0) (zero gradient) */
+#define CFD_BND_DOUBLEMACHUP 8      /* exact moving-shock state at the stage time */
+#define CFD_BND_SYMMETRYX 10        /* mirror, u negated */
+#define CFD_BND_SYMMETRYY 11        /* mirror, v negated */
+#define CFD_BND_SYMMETRYZ 12        /* extension for 3D: mirror, w negated */
+#define CFD_BND_PERIODIC_WRAP 100   /* extension: PERIODIC1D wired as a true wrap
+                                       (low side copies the far end, high side the near end) */
+
+typedef struct cfd_config {
+    int dim;            /* 1, 2 or 3 */
+    int n[3];           /* cells per direction (Info::icMax()); 1 for unused directions */
+    double h[3];        /* spacing per direction; the reference uses one h for all (Info::geth) */
+    double x0[3];       /* lower corner of the domain (Info::calZone[0,2,4]) */
+    int n_ghost;        /* must be 4 (Info::nGhostCell for WCNS5 + MND6, info.cpp:11) */
+    double gamma;       /* must be 1.4 (macro.hpp:28 GAMMA) */
+    int inter_method;   /* InterMethod enum value (macro.hpp:37-78) */
+    int flux_method;    /* CFD_FLUX_HLLC or CFD_FLUX_ROE */
+    int diff_method;    /* CFD_DIFF_MND6 */
+    int precision;      /* CFD_PREC_FP64 or CFD_PREC_MIXED */
+    int strict;         /* 1: reference operation order, no FMA contraction (bitwise parity build) */
+    int bc[3][2];       /* default boundary type per direction and side (0 = low, 1 = high),
+                           wired per line like Initializer::initBnds (initializer.cpp:743-870):
+                           low side i0 = first cell, offset = +stride (calOffset);
+                           high side i0 = last cell, offset = -stride (calOffsetInverse) */
+    int device;         /* CUDA device ordinal */
+    int seg_len[3];     /* cells per CTA segment along each sweep (0 = autotuned default) */
+} cfd_config;
+
+typedef struct cfd_handle cfd_handle;
+
+/* Fills *cfg with the reference's defaults (2D, 4 ghosts, gamma 1.4, WCNS5,
+ * HLLC, MND6, FP64, supersonic outlets on every side). */
+void cfd_config_default(cfd_config *cfg);
+
+/* Replaces BlockSolver(Info*)'s setup (blockSolver.cpp:24-41) for the device
+ * side: allocates the state, RHS and boundary tables. */
+int cfd_create(const cfd_config *cfg, cfd_handle **out);
+void cfd_destroy(cfd_handle *h);
+const char *cfd_last_error(const cfd_handle *h);
+
+/* Rewires one ghost strip, mirroring OneDBnd (oneDBnd.cpp:3-29):
+ * idim 1/2/3 selects x/y/z lines as in Bnds::getOneDBnd (bnds.cpp:3-21), (i, j)
+ * are the line's transverse indices, side 0/1 = low/high end. i0/offset are
+ * OneDBnd::setUpdate's source cell and stride; ghost_prim (n_ghost*nvar
+ * primitive values, may be NULL) is OneDBnd::setValue's static data. */
+int cfd_set_line_bc(cfd_handle *h, int idim, int i, int j, int side, int bnd_type, long long i0, int offset,
+                    const double *ghost_prim);
+
+/* Host <-> device state copies in the reference AoS layout (Data). */
+int cfd_upload_cons(cfd_handle *h, const double *aos);
+int cfd_download_cons(cfd_handle *h, double *aos);
+/* Primitive variables of the current state (Equation::consToPrim). */
+int cfd_download_prim(cfd_handle *h, double *aos);
+
+/* One RHS evaluation on the current state at time t (one stage body of
+ * RK3_SSP: consToPrim, Bnds::update, rhsSolve), written to aos_rhs in the
+ * reference layout. */
+int cfd_rhs(cfd_handle *h, double t, double *aos_rhs);
+
+/* CFL step of BlockSolver::getTimeIntervalExplicit: cfl / sum_d max_i
+ * ((sqrt(gamma p / rho) + |u_d|) / h_d) on the current state. */
+int cfd_max_dt(cfd_handle *h, double cfl, double *dt);
+
+/* One SSP-RK3 step of size dt starting at time t (BlockSolver::RK3_SSP; the
+ * stage times are t, t + dt, t + dt/2). If rho_linf is not NULL it receives
+ * max |R_rho| of the third stage (the reference's log value). */
+int cfd_rk3_step(cfd_handle *h, double dt, double t, double *rho_linf);
+
+/* Device-resident time loop of BlockSolver::stepsLoopCFL
+ * (blockSolver.cpp:170-235): from time *t, takes CFL steps clipped to the
+ * output interval until end_step output intervals are done or max_steps RK3
+ * steps were taken. dt and the clipping stay on the device; steps are launched
+ * as captured CUDA graphs. *t and *nsteps receive the final time and step
+ * count; dts/linf (length max_steps, may be NULL) receive per-step dt and
+ * max |R_rho|. */
+int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_steps, double *t, int *nsteps,
+            double *dts, double *linf);
+
+/* Device pointers and CUDA stream of the handle, for callers that keep the
+ * state resident (e.g. a framework tensor sharing the buffer). state receives
+ * the current conserved state in the device layout: planar SoA
+ * state[var * ncell + cell]. */
+int cfd_device_state(cfd_handle *h, double **state, long long *ncell, void **stream);
+/* Uploads/downloads a planar SoA device buffer (same layout as above). */
+int cfd_set_state_device(cfd_handle *h, const double *soa_dev);
+
+/* Pointwise known-answer hooks: evaluate the device interpolator for
+ * inter_method on n five-point stencils (q[5*i..5*i+4] -> out[i]), and the
+ * device Riemann flux on n face pairs (lr[2*nvar*i ...] = left prim | right
+ * prim -> out[nvar*i ...]) for sweep axis ax. Host pointers; used by tests. */
+int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double *out);
+int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr, int n, double *out);
+
+/* Library version string. */
+const char *cfd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDGPU_H */

@@ -1,0 +1,190 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of oracle/_ref/libcongfd_ref.so: the reference zone_FD solver
+compiled unmodified from its own sources (zone_FD/src/src/*.cpp) by
+oracle/Makefile, plus the C harness in oracle/ref_capi.cpp. Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg may use this module;
+the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libcongfd_ref.so"
+
+
+class RefCfg(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("zone", C.c_double * 6), ("inter_method", C.c_int),
+                ("flux_method", C.c_int), ("n_case", C.c_int), ("cfl", C.c_double)]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not REF_LIB.exists():
+            raise RuntimeError(f"{REF_LIB} missing: run `make -C oracle` where the reference sources are present")
+        lib = C.CDLL(str(REF_LIB))
+        vp = C.c_void_p
+        d = C.c_double
+        protos = {
+            "ref_create": (vp, [C.POINTER(RefCfg)]),
+            "ref_destroy": (None, [vp]),
+            "ref_ncells": (C.c_int, [vp]),
+            "ref_nvar": (C.c_int, [vp]),
+            "ref_h": (d, [vp, C.c_int]),
+            "ref_time": (d, [vp]),
+            "ref_set_time": (None, [vp, d]),
+            "ref_set_cons": (None, [vp, vp]),
+            "ref_get_cons": (None, [vp, vp]),
+            "ref_get_prim": (None, [vp, vp]),
+            "ref_rhs": (None, [vp, vp]),
+            "ref_max_dt": (d, [vp]),
+            "ref_rk3": (None, [vp, d]),
+            "ref_rho_linf": (d, [vp]),
+            "ref_run": (C.c_int, [vp, C.c_int, d, C.c_int, vp, vp]),
+            "ref_set_line_bc": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp]),
+            "ref_inter5": (d, [C.c_int, vp]),
+            "ref_flux2d": (None, [C.c_int, vp, C.c_int, vp]),
+            "ref_flux1d": (None, [C.c_int, vp, vp]),
+            "ref_set_threads": (None, [C.c_int]),
+        }
+        for name, (res, args) in protos.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"] and a.dtype == np.float64
+    return C.c_void_p(a.ctypes.data)
+
+
+class RefSolver:
+    """The reference BlockSolver driven through the harness.
+
+    dim/n: grid (cells); zone: Info::calZone; n_case selects the reference's
+    initial state and boundary wiring (Initializer); periodic=True rewires every
+    line end to a true wrap (PERIODIC1D with i0/offset pointing at the far end).
+    """
+
+    def __init__(self, dim, n, zone, inter_method=2, flux_method=0, n_case=0, cfl=0.5, periodic=False, threads=None):
+        self.lib = load()
+        if threads is not None:
+            self.lib.ref_set_threads(int(threads))
+        n3 = list(n) + [1] * (3 - len(n))
+        cfg = RefCfg(dim, (C.c_int * 3)(*n3), (C.c_double * 6)(*zone), inter_method, flux_method, n_case, cfl)
+        self.h = self.lib.ref_create(C.byref(cfg))
+        self.dim = dim
+        self.n = n3
+        self.ncell = self.lib.ref_ncells(self.h)
+        self.nvar = self.lib.ref_nvar(self.h)
+        if periodic:
+            self.wire_periodic()
+
+    def close(self):
+        if self.h:
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def wire_periodic(self):
+        nx, ny = self.n[0], self.n[1]
+        if self.dim == 1:
+            self.lib.ref_set_line_bc(self.h, 1, 0, 0, 0, 1, nx - 1, -1, None)
+            self.lib.ref_set_line_bc(self.h, 1, 0, 0, 1, 1, 0, 1, None)
+            return
+        for j in range(ny):
+            self.lib.ref_set_line_bc(self.h, 1, j, 0, 0, 1, j * nx + nx - 1, -1, None)
+            self.lib.ref_set_line_bc(self.h, 1, j, 0, 1, 1, j * nx, 1, None)
+        for i in range(nx):
+            self.lib.ref_set_line_bc(self.h, 2, i, 0, 0, 1, i + (ny - 1) * nx, -nx, None)
+            self.lib.ref_set_line_bc(self.h, 2, i, 0, 1, 1, i, nx, None)
+
+    def set_line_bc(self, idim, i, j, side, typ, i0, offset, values=None):
+        v = None if values is None else np.ascontiguousarray(np.broadcast_to(np.asarray(values, float), (4, self.nvar)))
+        rc = self.lib.ref_set_line_bc(self.h, idim, i, j, side, int(typ), int(i0), int(offset),
+                                      _p(v) if v is not None else None)
+        assert rc == 0
+
+    @property
+    def cons(self) -> np.ndarray:
+        a = np.empty((self.ncell, self.nvar))
+        self.lib.ref_get_cons(self.h, _p(a))
+        return a
+
+    @cons.setter
+    def cons(self, v):
+        a = np.ascontiguousarray(v, dtype=np.float64).reshape(self.ncell, self.nvar)
+        self.lib.ref_set_cons(self.h, _p(a))
+
+    @property
+    def prim(self) -> np.ndarray:
+        a = np.empty((self.ncell, self.nvar))
+        self.lib.ref_get_prim(self.h, _p(a))
+        return a
+
+    @property
+    def t(self) -> float:
+        return self.lib.ref_time(self.h)
+
+    @t.setter
+    def t(self, v):
+        self.lib.ref_set_time(self.h, float(v))
+
+    def rhs(self) -> np.ndarray:
+        a = np.empty((self.ncell, self.nvar))
+        self.lib.ref_rhs(self.h, _p(a))
+        return a
+
+    def max_dt(self) -> float:
+        return self.lib.ref_max_dt(self.h)
+
+    def solve(self, dt: float) -> float:
+        self.lib.ref_rk3(self.h, float(dt))
+        return self.lib.ref_rho_linf(self.h)
+
+    def run(self, end_step: int, output_dt: float, max_steps: int = 1 << 22):
+        dts = np.zeros(max_steps)
+        lin = np.zeros(max_steps)
+        k = self.lib.ref_run(self.h, end_step, output_dt, max_steps, _p(dts), _p(lin))
+        return dts[:k], lin[:k]
+
+
+def ref_inter5(inter_method: int, q: np.ndarray) -> np.ndarray:
+    lib = load()
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return np.array([lib.ref_inter5(inter_method, C.c_void_p(q[i].ctypes.data)) for i in range(q.shape[0])])
+
+
+def ref_flux(dim: int, ax: int, flux_method: int, lr: np.ndarray) -> np.ndarray:
+    lib = load()
+    lr = np.ascontiguousarray(lr, dtype=np.float64)
+    nv = dim + 2
+    out = np.empty((lr.shape[0], nv))
+    for i in range(lr.shape[0]):
+        row = np.ascontiguousarray(lr[i])
+        o = np.empty(nv)
+        if dim == 1:
+            lib.ref_flux1d(flux_method, _p(row), _p(o))
+        else:
+            lib.ref_flux2d(flux_method, _p(row), int(ax == 1), _p(o))
+        out[i] = o
+    return out
