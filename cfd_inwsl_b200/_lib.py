@@ -75,6 +75,9 @@ _PROTOS = {
     "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_version": (C.c_char_p, []),
+    "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_launch_count": (C.c_ulonglong, [C.c_void_p]),
+    "cfd_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double]),
 }
 
 

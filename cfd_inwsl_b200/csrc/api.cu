@@ -74,6 +74,45 @@ __global__ void __launch_bounds__(256) wave_speed_kernel(const double *__restric
     cfd::block_max_reduce<256, 4>(0.0, lam, red);
 }
 
+// Step control of stepsLoopCFL (blockSolver.cpp:176-201) on the device: the
+// loop test, dt = CFL / sum_d lambda_d from the wave-speed maxima of the
+// current state, clipping to the output interval, stage coefficients.
+__global__ void step_begin_kernel(cfd::StepCtl *c, const unsigned long long *red, int dim, double *dts)
+{
+    if (c->done) return;
+    if (!(c->step < c->endStep && c->k < c->maxSteps)) {
+        c->done = 1;
+        return;
+    }
+    double lambda = 0;
+    for (int d = 0; d < dim; d++) lambda += __longlong_as_double((long long)red[1 + d]);
+    double dt = c->cfl / lambda;
+    if (c->outputT + dt > c->outputDt) {
+        dt = c->outputDt - c->outputT;
+        c->outputT = 0.0;
+        c->step++;
+    } else
+        c->outputT += dt;
+    c->dt = dt;
+    c->bdt[1] = dt;
+    c->bdt[2] = 0.25 * dt;
+    c->bdt[3] = 2.0 / 3.0 * dt;
+    c->tst[1] = c->t;
+    c->tst[2] = c->t + dt;
+    c->tst[3] = c->tst[2] - dt / 2;
+    if (dts) dts[c->k] = dt;
+}
+
+// BlockSolver::solve's time update and the per-step log value (rhoLinf).
+__global__ void step_end_kernel(cfd::StepCtl *c, const unsigned long long *red, double *linf)
+{
+    if (c->done) return;
+    if (linf) linf[c->k] = __longlong_as_double((long long)red[0]);
+    double dt = c->dt;
+    c->t = (((c->t + dt) - dt / 2) - dt / 2) + dt;
+    c->k++;
+}
+
 // Pointwise test kernels.
 template <int FAM>
 __global__ void eval_inter5_kernel(const double *q, int n, double c, double *out)
@@ -161,9 +200,19 @@ struct cfd_handle {
     bool ws_valid = false;       // red[1..3] hold the wave speeds of the current state
     double dm_u = 0.0, dm_v = 0.0;
     std::string msg;
+    cudaStream_t own_stream = nullptr;   // created by cfd_create
+    cfd::StepCtl *ctl = nullptr;         // device step control
+    cfd::StepCtl *ctl_host = nullptr;    // pinned mirror
+    double *d_dts = nullptr, *d_linf = nullptr;
+    int log_cap = 0;
+    // captured step graphs, by (steps per graph index: 1, 3, 12) x (start slot)
+    cudaGraphExec_t graph[3][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    unsigned long long launches = 0;     // kernels this library launched
 };
 
 namespace {
+
+void drop_graphs(cfd_handle *h);
 
 int fail(cfd_handle *h, int code, const std::string &m)
 {
@@ -262,6 +311,7 @@ int sync_bc(cfd_handle *h)
     if (!h->bc_vals.empty()) {
         size_t bytes = h->bc_vals.size() * sizeof(double);
         if (bytes > h->d_bcvals_cap) {
+            drop_graphs(h);
             if (h->d_bcvals) cudaFree(h->d_bcvals);
             h->d_bcvals = nullptr;
             CFD_CUDA(h, cudaMalloc(&h->d_bcvals, bytes));
@@ -290,6 +340,7 @@ int launch_aos_to_soa(cfd_handle *h, const double *aos, double *soa)
     else if (h->nv == 4) aos_to_soa_kernel<4><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
     else aos_to_soa_kernel<5><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
     CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
     return CFD_OK;
 }
 
@@ -300,6 +351,7 @@ int launch_soa_to_aos(cfd_handle *h, const double *soa, double *aos, int to_prim
     else if (h->nv == 4) soa_to_aos_kernel<4><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
     else soa_to_aos_kernel<5><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
     CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
     return CFD_OK;
 }
 
@@ -330,6 +382,7 @@ int sweep(cfd_handle *h, int d, const SweepParams &p)
 {
     cudaError_t e = cfd::launch_sweep_any(h->strict, h->nv, h->fam, d, h->cfg.flux_method, p, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "sweep kernel launch");
+    h->launches++;
     return CFD_OK;
 }
 
@@ -351,7 +404,7 @@ int rhs_all(cfd_handle *h, const double *u, double t)
 
 // One RK stage: RHS of uin, then uout = combination (blockSolver.cpp:51-86).
 int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, double *uout, double A, double Bdt,
-             double C, double t, bool reduce)
+             double C, double t, bool reduce, const cfd::StepCtl *ctl = nullptr)
 {
     for (int d = 0; d < h->dim; d++) {
         SweepParams p = base_params(h, d);
@@ -368,6 +421,7 @@ int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, doub
         p.rkC = C;
         p.want_reduce = (reduce && last) ? 1 : 0;
         p.t = t;
+        p.ctl = ctl;
         int rc = sweep(h, d, p);
         if (rc) return rc;
     }
@@ -386,6 +440,95 @@ int default_seg_len(const cfd_handle *h, int d)
     int seg = n;
     while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
     return seg;
+}
+
+
+void drop_graphs(cfd_handle *h)
+{
+    for (int g = 0; g < 3; g++)
+        for (int k = 0; k < 3; k++) {
+            if (h->graph[g][k]) cudaGraphExecDestroy(h->graph[g][k]);
+            h->graph[g][k] = nullptr;
+        }
+}
+
+constexpr int kGraphSteps[3] = {1, 3, 12};
+
+int check_err(cfd_handle *h, unsigned err)
+{
+    if (err & cfd::ERR_NONFINITE) return fail(h, CFD_ERR_NONFINITE, "non-finite value in the state after an RK3 step");
+    if (err & cfd::ERR_NEGATIVE) return fail(h, CFD_ERR_NEGATIVE_STATE, "density or pressure <= 0 after an RK3 step");
+    return CFD_OK;
+}
+
+int launch_wave_speed(cfd_handle *h)
+{
+    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
+    int g = grid_for(h->ncell);
+    const double *u = h->u[h->cur];
+    if (h->nv == 3) wave_speed_kernel<3><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+    else if (h->nv == 4) wave_speed_kernel<4><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+    else wave_speed_kernel<5><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    h->ws_valid = true;
+    return CFD_OK;
+}
+
+int ensure_run_buffers(cfd_handle *h, int max_steps)
+{
+    if (!h->ctl) {
+        CFD_CUDA(h, cudaMalloc(&h->ctl, sizeof(cfd::StepCtl)));
+        CFD_CUDA(h, cudaMallocHost(&h->ctl_host, sizeof(cfd::StepCtl)));
+    }
+    if (max_steps > h->log_cap) {
+        cudaFree(h->d_dts);
+        cudaFree(h->d_linf);
+        h->d_dts = h->d_linf = nullptr;
+        int cap = max_steps + 16;  // steps past the end stay inside the buffers
+        CFD_CUDA(h, cudaMalloc(&h->d_dts, sizeof(double) * cap));
+        CFD_CUDA(h, cudaMalloc(&h->d_linf, sizeof(double) * cap));
+        h->log_cap = max_steps;
+        drop_graphs(h);
+    }
+    return CFD_OK;
+}
+
+// Enqueue one device-controlled SSP-RK3 step (buffers by role).
+int enqueue_step(cfd_handle *h, int cur)
+{
+    double *U0 = h->u[cur], *U1 = h->u[(cur + 1) % 3], *U2 = h->u[(cur + 2) % 3];
+    step_begin_kernel<<<1, 1, 0, h->stream>>>(h->ctl, h->red, h->dim, h->d_dts);
+    CFD_CUDA(h, cudaGetLastError());
+    int rc;
+    if ((rc = rk_stage(h, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl))) return rc;
+    if ((rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl))) return rc;
+    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
+    if ((rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl))) return rc;
+    step_end_kernel<<<1, 1, 0, h->stream>>>(h->ctl, h->red, h->d_linf);
+    CFD_CUDA(h, cudaGetLastError());
+    return CFD_OK;
+}
+
+// Capture kGraphSteps[gi] device-controlled steps starting at state slot
+// `slot` into one CUDA graph (kept until the buffers change).
+int ensure_graph(cfd_handle *h, int gi, int slot)
+{
+    if (h->graph[gi][slot]) return CFD_OK;
+    const int G = kGraphSteps[gi];
+    unsigned long long saved = h->launches;
+    cudaGraph_t g;
+    CFD_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = CFD_OK;
+    for (int s = 0; s < G && rc == CFD_OK; s++) rc = enqueue_step(h, (slot + s) % 3);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = saved;
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->graph[gi][slot], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    return CFD_OK;
 }
 
 } // namespace
@@ -455,7 +598,8 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     };
     cudaError_t e;
     if ((e = cudaSetDevice(cfg->device)) != cudaSuccess) return bail(e, "cudaSetDevice");
-    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    h->stream = h->own_stream;
     size_t bytes = sizeof(double) * h->ncell * h->nv;
     for (int k = 0; k < 3; k++)
         if ((e = cudaMalloc(&h->u[k], bytes)) != cudaSuccess) return bail(e, "state");
@@ -495,7 +639,12 @@ void cfd_destroy(cfd_handle *h)
         cudaFree(h->d_bchi[d]);
     }
     cudaFree(h->d_bcvals);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaFree(h->ctl);
+    if (h->ctl_host) cudaFreeHost(h->ctl_host);
+    cudaFree(h->d_dts);
+    cudaFree(h->d_linf);
+    drop_graphs(h);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
 
@@ -580,13 +729,8 @@ int cfd_max_dt(cfd_handle *h, double cfl, double *dt)
     if (!h || !dt) return CFD_ERR_CONFIG;
     unsigned long long r[4];
     if (!h->ws_valid) {
-        CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
-        int g = grid_for(h->ncell);
-        const double *u = h->u[h->cur];
-        if (h->nv == 3) wave_speed_kernel<3><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-        else if (h->nv == 4) wave_speed_kernel<4><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-        else wave_speed_kernel<5><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-        CFD_CUDA(h, cudaGetLastError());
+        int rc = launch_wave_speed(h);
+        if (rc) return rc;
     }
     CFD_CUDA(h, cudaMemcpyAsync(r, h->red, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -621,39 +765,103 @@ int cfd_rk3_step(cfd_handle *h, double dt, double t, double *rho_linf)
     CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));
     if (rho_linf) std::memcpy(rho_linf, &r0, sizeof(double));
-    if (err & cfd::ERR_NONFINITE) return fail(h, CFD_ERR_NONFINITE, "non-finite value in the state after an RK3 step");
-    if (err & cfd::ERR_NEGATIVE) return fail(h, CFD_ERR_NEGATIVE_STATE, "density or pressure <= 0 after an RK3 step");
-    return CFD_OK;
+    return check_err(h, err);
 }
 
 int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_steps, double *t, int *nsteps,
             double *dts, double *linf)
 {
-    if (!h || !t || !nsteps) return CFD_ERR_CONFIG;
-    // stepsLoopCFL (blockSolver.cpp:170-235), one host round trip per step.
-    int step = 0, k = 0;
-    double outputT = 0.0;
-    int rc = CFD_OK;
-    while (step < end_step && k < max_steps) {
-        double dt;
-        if ((rc = cfd_max_dt(h, cfl, &dt))) return rc;
-        if (outputT + dt > output_dt) {
-            dt = output_dt - outputT;
-            outputT = 0.0;
-            step++;
-        } else
-            outputT += dt;
-        double l = 0.0;
-        rc = cfd_rk3_step(h, dt, *t, &l);
-        // BlockSolver::solve: RK3_SSP moves t by +dt, -dt/2, -dt/2, then t += dt
-        *t = (((*t + dt) - dt / 2) - dt / 2) + dt;
-        if (dts) dts[k] = dt;
-        if (linf) linf[k] = l;
-        k++;
-        if (rc) break;
+    if (!h || !t || !nsteps || max_steps < 0) return CFD_ERR_CONFIG;
+    *nsteps = 0;
+    if (max_steps == 0 || end_step <= 0) return CFD_OK;
+    int rc = sync_bc(h);
+    if (rc) return rc;
+    if ((rc = ensure_run_buffers(h, max_steps))) return rc;
+    if (!h->ws_valid && (rc = launch_wave_speed(h))) return rc;
+    // stepsLoopCFL state: step counts output intervals, outputT the time since the last one
+    cfd::StepCtl *c = h->ctl_host;
+    std::memset(c, 0, sizeof(*c));
+    c->t = *t;
+    c->outputT = 0.0;
+    c->outputDt = output_dt;
+    c->cfl = cfl;
+    c->endStep = end_step;
+    c->maxSteps = max_steps;
+    CFD_CUDA(h, cudaMemcpyAsync(h->ctl, c, sizeof(*c), cudaMemcpyHostToDevice, h->stream));
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+    const int cur0 = h->cur;
+    // Steps are launched as captured graphs of 12, 3 or 1 steps covering
+    // exactly max_steps; if the output-interval test ends the loop earlier the
+    // remaining launched steps are no-ops on the device. The host checks the
+    // device state between batches whose size doubles.
+    int launched = 0, slot = cur0, quota = 12;
+    const unsigned long long per_step = 2 + 3ULL * h->dim;
+    while (true) {
+        int target = launched + quota;
+        if (target > max_steps) target = max_steps;
+        while (launched < target) {
+            int rem = target - launched;
+            int gi = rem >= 12 ? 2 : rem >= 3 ? 1 : 0;
+            if ((rc = ensure_graph(h, gi, slot))) return rc;
+            CFD_CUDA(h, cudaGraphLaunch(h->graph[gi][slot], h->stream));
+            h->launches += per_step * kGraphSteps[gi];
+            launched += kGraphSteps[gi];
+            slot = (slot + kGraphSteps[gi]) % 3;
+        }
+        CFD_CUDA(h, cudaMemcpyAsync(c, h->ctl, sizeof(*c), cudaMemcpyDeviceToHost, h->stream));
+        CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (c->done || launched >= max_steps) break;
+        if (quota < (1 << 20)) quota *= 2;
     }
+    // a step that met the loop test before `done` was set still has to finish
+    int k = c->k;
     *nsteps = k;
-    return rc;
+    *t = c->t;
+    h->cur = (cur0 + k) % 3;
+    h->ws_valid = true;  // stage 3 of the last step left the wave speeds in red[1..3]
+    if (k > 0 && dts) CFD_CUDA(h, cudaMemcpy(dts, h->d_dts, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    if (k > 0 && linf) CFD_CUDA(h, cudaMemcpy(linf, h->d_linf, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    unsigned err;
+    CFD_CUDA(h, cudaMemcpy(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost));
+    return check_err(h, err);
+}
+
+int cfd_set_stream(cfd_handle *h, void *stream)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return CFD_OK;
+}
+
+unsigned long long cfd_launch_count(const cfd_handle *h) { return h ? h->launches : 0; }
+
+int cfd_sweep(cfd_handle *h, int idim, int mode, double t)
+{
+    if (!h) return CFD_ERR_CONFIG;
+    int d = idim - 1;
+    if (d < 0 || d >= h->dim || mode < 0 || mode > 2) return fail(h, CFD_ERR_CONFIG, "bad idim/mode");
+    int rc = sync_bc(h);
+    if (rc) return rc;
+    SweepParams p = base_params(h, d);
+    p.u = h->u[h->cur];
+    p.rhs = h->rhs;
+    p.t = t;
+    if (mode == 2) {
+        // the stage-2 combination into the next slot; the current state is kept
+        p.mode = cfd::MODE_RK;
+        p.first = 0;
+        p.rk_stage = 2;
+        p.u0 = h->u[h->cur];
+        p.u_out = h->u[(h->cur + 2) % 3];
+        p.rkA = 0.75;
+        p.rkBdt = 0.0;
+        p.rkC = 0.25;
+    } else {
+        p.mode = cfd::MODE_WRITE;
+        p.first = (mode == 0);
+    }
+    return sweep(h, d, p);
 }
 
 int cfd_device_state(cfd_handle *h, double **state, long long *ncell, void **stream)

@@ -42,7 +42,7 @@ __device__ __forceinline__ void load_cons_prim(const double *__restrict__ u, lon
 // Ghost cell k (0 = nearest the boundary) of a line end, as OneDBnd::update
 // leaves it after Bnds::update (oneDBnd.cpp:31-114).
 template <int NV>
-__device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &bl, int k, double *pr)
+__device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &bl, int k, double tstage, double *pr)
 {
     switch (bl.type) {
     case BND_PERIODIC1D:
@@ -70,7 +70,7 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
         // from 0, not from the line end) and x is the edge cell's centre.
         double x = bl.coor_x;
         double y = -bl.dh_y / 2 + k * bl.dh_y;
-        double gt = 1.0 / 6.0 + sqrt(3.0) / 3.0 * (1.0 + 20 * p.t);
+        double gt = 1.0 / 6.0 + sqrt(3.0) / 3.0 * (1.0 + 20 * tstage);
         if (y > sqrt(3.0) * (x - gt)) {
             pr[0] = 8.0; pr[1] = p.dm_u; pr[2] = p.dm_v; pr[NV - 1] = 116.5;
         } else {
@@ -102,6 +102,10 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
     constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
+    // device-resident loop: the whole launch is a no-op once the loop is done
+    if (p.ctl && p.ctl->done) return;
+    const double tstage = p.ctl ? p.ctl->tst[p.rk_stage] : p.t;
+    const double rkBdt = p.ctl ? p.ctl->bdt[p.rk_stage] : p.rkBdt;
     extern __shared__ double smem[];
     double *sp = smem;                   // [NV][W][LSP] prim
     double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue)
@@ -146,10 +150,10 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
             load_cons_prim<NV>(p.u, p.ncell, base + (long long)P * sAX, pr);
         } else if (P < 0) {
             int k = -P - 1;
-            ghost_prim<NV>(p, p.bc_lo[lid], k > 3 ? 3 : k, pr);
+            ghost_prim<NV>(p, p.bc_lo[lid], k > 3 ? 3 : k, tstage, pr);
         } else {
             int k = P - nd;
-            ghost_prim<NV>(p, p.bc_hi[lid], k > 3 ? 3 : k, pr);
+            ghost_prim<NV>(p, p.bc_hi[lid], k > 3 ? 3 : k, tstage, pr);
         }
         double cs[NV];
         prim_to_cons<NV>(pr, cs);
@@ -233,9 +237,9 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
                     if (v == 0 && p.want_reduce) red_rho = fmax(red_rho, fabs(r));
                     double o;
                     if (p.rk_stage == 1) {
-                        o = p.u0[gi] - p.rkBdt * r;
+                        o = p.u0[gi] - rkBdt * r;
                     } else {
-                        o = p.rkA * p.u0[gi] - p.rkBdt * r + p.rkC * p.u[gi];
+                        o = p.rkA * p.u0[gi] - rkBdt * r + p.rkC * p.u[gi];
                     }
                     uo[v] = o;
                     p.u_out[gi] = o;

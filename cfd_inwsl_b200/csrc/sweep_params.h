@@ -34,6 +34,16 @@ struct BcLine {
 enum SweepMode : int { MODE_WRITE = 0, MODE_RK = 2 };
 enum ErrBits : unsigned { ERR_NONFINITE = 1u, ERR_NEGATIVE = 2u, ERR_TIMEOUT = 4u };
 
+// Device-resident state of the time loop of BlockSolver::stepsLoopCFL
+// (blockSolver.cpp:170-235), advanced by single-thread control kernels so that
+// whole steps can be captured in CUDA graphs without host round trips.
+struct StepCtl {
+    double t, outputT, outputDt, cfl, dt;
+    double bdt[4];   // per stage: dt, 0.25*dt, (2/3)*dt (index = stage)
+    double tst[4];   // stage times t, t+dt, (t+dt)-dt/2
+    int step, endStep, k, maxSteps, done, pad;
+};
+
 struct SweepParams {
     const double *u;    // current state U_k, planar SoA u[v * ncell + cell]
     const double *u0;   // RK base state U_0
@@ -54,7 +64,8 @@ struct SweepParams {
     const BcLine *bc_lo;  // per line (index a + n[T0] * b), low end
     const BcLine *bc_hi;  // per line, high end
     const double *bc_vals; // static ghost prim values [slot][4][NV]
-    double t;           // stage time
+    double t;           // stage time (ignored when ctl is set)
+    const StepCtl *ctl; // device-resident step control (null: use rkBdt/t)
     double dm_u, dm_v;  // DoubleMachUp post-shock velocity, 8.25 cos(pi/6) and -8.25 sin(pi/6) from the host libm
     double icst;        // interpolator constant (TENO cutoff)
     int seg_len;        // cells per CTA segment along the sweep

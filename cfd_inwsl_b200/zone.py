@@ -20,7 +20,6 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
-import math
 
 import numpy as np
 
@@ -296,11 +295,9 @@ class BlockSolver:
         """BlockSolver::stepsLoopCFL (blockSolver.cpp:170-235) without output files:
         steps until info.step reaches info.endStep. Returns (dts, linfs) if record."""
         info = self.info
-        eps = 1e-15
         dts, linfs = [], []
         k = 0
         while info.step < info.endStep and k < max_steps:
-            _ = eps
             dt = self.getTimeIntervalExplicit()
             if info.outputT + dt > info.outputDt:
                 dt = info.outputDt - info.outputT
@@ -362,5 +359,3 @@ def prim_to_cons(prim: np.ndarray) -> np.ndarray:
     out[..., nv - 1] = p / (GAMMA - 1) + 0.5 * r * np.sum(vel * vel, axis=-1)
     return out
 
-
-_ = math

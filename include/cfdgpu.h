@@ -146,6 +146,21 @@ int cfd_device_state(cfd_handle *h, double **state, long long *ncell, void **str
 /* Uploads/downloads a planar SoA device buffer (same layout as above). */
 int cfd_set_state_device(cfd_handle *h, const double *soa_dev);
 
+/* Runs the handle's work on a caller-provided CUDA stream (cudaStream_t passed
+ * as void*; NULL restores the handle's own stream). The caller keeps ownership. */
+int cfd_set_stream(cfd_handle *h, void *stream);
+
+/* Number of kernels this library launched for the handle so far (every kernel
+ * of a captured step graph counts once per graph launch). */
+unsigned long long cfd_launch_count(const cfd_handle *h);
+
+/* One direction's line sweep alone, stream-ordered and not synchronised (the
+ * per-kernel timing hook of the benchmark). idim is 1-based. mode 0: RHS of
+ * this direction into the RHS buffer; 1: added to the RHS buffer; 2: added and
+ * combined like RK stage 2 (dt = 0) into a spare state slot, as the last sweep
+ * of a stage runs. The current state is not changed. */
+int cfd_sweep(cfd_handle *h, int idim, int mode, double t);
+
 /* Pointwise known-answer hooks: evaluate the device interpolator for
  * inter_method on n five-point stencils (q[5*i..5*i+4] -> out[i]), and the
  * device Riemann flux on n face pairs (lr[2*nvar*i ...] = left prim | right

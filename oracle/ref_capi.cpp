@@ -220,6 +220,10 @@ double ref_inter5(int inter_method, const double *q5)
     case WCNS5CONGZCT4: return Teno5_CongZCT4(q);
     case WCNS5CONGZCT7: return Teno5_CongZCT7(q);
     case new_TCNS5: return new_Teno5_Z(q);
+    case new_WCNS5CONGZ: return new_Teno5_CongZ(q);
+    case congTCNS5CT5: return congTcns5_ZCT5(q);
+    case congTCNS5CT10: return congTcns5_ZCT10(q);
+    case MUCSLIN5: return musclIn5(q);
     default: return NAN;
     }
 }

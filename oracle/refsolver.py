@@ -188,3 +188,67 @@ def ref_flux(dim: int, ax: int, flux_method: int, lr: np.ndarray) -> np.ndarray:
             lib.ref_flux2d(flux_method, _p(row), int(ax == 1), _p(o))
         out[i] = o
     return out
+
+
+# ---------------------------------------------------------------- C restatement
+ORC_LIB = HERE / "_ref" / "libcfd_oracle.so"
+ORC_OUTLET, ORC_SYMMETRY, ORC_WRAP, ORC_MIRRORCOPY = 7, 10, 100, 1
+# InterMethod -> (family, constant), as the library's selector maps it
+ORC_FAMILY = {2: (0, 0.0), 3: (1, 0.0), 11: (2, 1e-5), 12: (2, 1e-4), 13: (2, 1e-7), 22: (2, 1e-5),
+              23: (2, 1e-10), 35: (2, 1e-5), 8: (3, 0.15704178024750198), 37: (3, 0.15704178024750198),
+              9: (3, 0.23050581003334941), 10: (3, 0.072892337360747711), 15: (4, 0.0)}
+
+
+class OrcCfg(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("h", C.c_double), ("fam", C.c_int), ("icst", C.c_double),
+                ("flux", C.c_int), ("bc", (C.c_int * 2) * 3), ("threads", C.c_int)]
+
+
+_orc = None
+
+
+def orc_load() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORC_LIB.exists():
+            raise RuntimeError(f"{ORC_LIB} missing: run `make -C oracle`")
+        lib = C.CDLL(str(ORC_LIB))
+        vp = C.c_void_p
+        lib.orc_rhs.argtypes = [C.POINTER(OrcCfg), vp, vp]
+        lib.orc_rhs.restype = None
+        lib.orc_max_dt.argtypes = [C.POINTER(OrcCfg), vp, C.c_double]
+        lib.orc_max_dt.restype = C.c_double
+        lib.orc_rk3.argtypes = [C.POINTER(OrcCfg), vp, C.c_double]
+        lib.orc_rk3.restype = C.c_double
+        lib.orc_inter5.argtypes = [C.c_int, C.c_double, vp]
+        lib.orc_inter5.restype = C.c_double
+        _orc = lib
+    return _orc
+
+
+class OracleC:
+    """The plain-C restatement (1D/2D/3D) on a uniform grid with per-side BC kinds."""
+
+    def __init__(self, dim, n, h, inter_method=2, flux_method=0, bc=None, threads=0):
+        self.lib = orc_load()
+        fam, icst = ORC_FAMILY[inter_method]
+        n3 = list(n) + [1] * (3 - len(n))
+        bcs = bc if bc is not None else [[ORC_OUTLET] * 2] * 3
+        arr = ((C.c_int * 2) * 3)(*[(C.c_int * 2)(*bcs[d]) for d in range(3)])
+        self.cfg = OrcCfg(dim, (C.c_int * 3)(*n3), h, fam, icst, flux_method, arr, threads)
+        self.nvar = dim + 2
+        self.ncell = n3[0] * n3[1] * n3[2]
+        self.cons = None
+
+    def rhs(self, cons=None) -> np.ndarray:
+        u = np.ascontiguousarray(self.cons if cons is None else cons, dtype=np.float64)
+        out = np.empty((self.ncell, self.nvar))
+        self.lib.orc_rhs(C.byref(self.cfg), _p(u), _p(out))
+        return out
+
+    def max_dt(self, cfl) -> float:
+        return self.lib.orc_max_dt(C.byref(self.cfg), _p(np.ascontiguousarray(self.cons)), cfl)
+
+    def solve(self, dt) -> float:
+        self.cons = np.ascontiguousarray(self.cons, dtype=np.float64).copy()
+        return self.lib.orc_rk3(C.byref(self.cfg), _p(self.cons), float(dt))

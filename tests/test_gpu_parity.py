@@ -1,0 +1,342 @@
+"""GPU path (libcfdgpu.so through the C ABI) against the reference and the oracle.
+
+Tolerances: the strict flavour (reference operation order, no FMA) must match
+the reference bit for bit; the fast flavour within 1e-12 relative L-inf after
+one RHS / one RK3 step and 1e-10 after full smooth runs.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cfd_inwsl_b200 import _lib, zone
+from tests.util import gpu_solver, quadrant_state, rel_linf, smooth_state_3d
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL_STEP = 1e-12
+TOL_RUN = 1e-10
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    from tests.conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+
+
+# ----------------------------------------------------------------- pointwise KATs
+def test_interpolators_bitwise_against_reference():
+    g = np.load(GOLD / "kat_inter5.npz")
+    for key in g.files:
+        if key.startswith("m"):
+            out = _lib.eval_inter5(int(key[1:]), g["q"])
+            np.testing.assert_array_equal(out, g[key], err_msg=key)
+
+
+def test_riemann_fluxes_bitwise_against_reference():
+    g = np.load(GOLD / "kat_flux.npz")
+    for key in g.files:
+        if key.startswith("f"):
+            dim = int(key[1])
+            fm = int(key.split("_fm")[1][0])
+            ax = int(key[-1])
+            out = _lib.eval_flux(dim, ax, fm, g[f"lr{dim}d"])
+            np.testing.assert_array_equal(out, g[key], err_msg=key)
+
+
+@pytest.mark.parametrize("fm", [0, 1])
+def test_flux_mirror_symmetry(fm):
+    """symmetrytest.cpp: the y-normal flux of a state equals the x-normal flux of
+    its mirror image (u and v exchanged), bit for bit; also for the 3D fluxes."""
+    rng = np.random.default_rng(11)
+    n = 300
+    L = np.column_stack([rng.uniform(0.1, 2, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(0.1, 2, n)])
+    R = np.column_stack([rng.uniform(0.1, 2, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(0.1, 2, n)])
+    sw = [0, 2, 1, 3]
+    fx = _lib.eval_flux(2, 0, fm, np.concatenate([L, R], 1))
+    fy = _lib.eval_flux(2, 1, fm, np.concatenate([L[:, sw], R[:, sw]], 1))
+    np.testing.assert_array_equal(fx, fy[:, sw])
+    L3 = np.column_stack([L[:, :3], rng.uniform(-1, 1, n), L[:, 3]])
+    R3 = np.column_stack([R[:, :3], rng.uniform(-1, 1, n), R[:, 3]])
+    for ax, perm in ((1, [0, 2, 1, 3, 4]), (2, [0, 3, 2, 1, 4])):
+        f0 = _lib.eval_flux(3, 0, fm, np.concatenate([L3, R3], 1))
+        fa = _lib.eval_flux(3, ax, fm, np.concatenate([L3[:, perm], R3[:, perm]], 1))
+        np.testing.assert_allclose(fa[:, perm], f0, rtol=1e-15, atol=1e-15)
+
+
+# ----------------------------------------------------------------- 2D against the reference fixtures
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_rhs_dt_step_2d_golden(strict):
+    g = np.load(GOLD / "rhs_2d.npz")
+    for k, n, im, fm, ncase, periodic in g["meta"]:
+        s = gpu_solver(2, [n, n], im=int(im), fm=int(fm), strict=strict, ncase=int(ncase), periodic=bool(periodic))
+        s.set_cons(g[f"c{k}_cons"])
+        rhs = s.rhsSolve()
+        dt_ref, linf_ref = g[f"c{k}_dt"]
+        dt = s.getTimeIntervalExplicit()
+        linf = s.solve(dt_ref)
+        if strict:
+            np.testing.assert_array_equal(rhs, g[f"c{k}_rhs"], err_msg=f"case {k}")
+            assert dt == dt_ref and linf == linf_ref
+            np.testing.assert_array_equal(s.cons, g[f"c{k}_step"])
+        else:
+            assert rel_linf(rhs, g[f"c{k}_rhs"]) < TOL_STEP, k
+            assert abs(dt - dt_ref) <= 1e-14 * dt_ref
+            assert rel_linf(s.cons, g[f"c{k}_step"]) < TOL_STEP
+        s.close()
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_sod_400_full_run(strict):
+    """Sod, 400 cells, WCNS5 + HLLC, CFL 0.5 to t = 0.2, point by point."""
+    g = np.load(GOLD / "sod_400.npz")
+    s = gpu_solver(1, [400], [-0.5, 0.5, 0, 0, 0, 0], im=2, fm=0, strict=strict)
+    s.set_cons(g["cons0"])
+    s.info.endStep = 1
+    s.info.outputDt = 0.2
+    dts, lin = s.stepsLoopCFL(record=True)
+    assert len(dts) == len(g["dts"]) == 349
+    if strict:
+        np.testing.assert_array_equal(dts, g["dts"])
+        np.testing.assert_array_equal(s.cons, g["cons"])
+    else:
+        assert rel_linf(s.cons, g["cons"]) < TOL_RUN
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_reference_sod_log_on_gpu(strict):
+    log = np.array(json.loads((GOLD / "sod_congtcns5ct5_101.json").read_text())["rows"])
+    s = gpu_solver(1, [100], [-0.5, 0.5, 0, 0, 0, 0], im=22, fm=0, strict=strict)
+    s.set_cons(zone.sod_1d(s.info))
+    s.info.endStep = 2
+    s.info.outputDt = 0.1
+    dts, lin = s.stepsLoopCFL(record=True)
+    assert len(dts) == 86
+    assert np.all(np.round(dts, 10) == log[:86, 1])
+    assert np.all(np.round(lin, 4) == log[:86, 2])
+
+
+# ----------------------------------------------------------------- live reference comparisons
+@pytest.mark.parametrize("im,fm", [(2, 0), (11, 1), (35, 0), (8, 1), (3, 0), (15, 1), (10, 0), (23, 1)])
+def test_random_quadrants_10_steps_vs_reference(ref, im, fm):
+    rng = np.random.default_rng(100 + im)
+    n = 48
+    c = quadrant_state(n, rng)
+    r = ref.RefSolver(2, [n, n], [0, 1, 0, 1, 0, 0], inter_method=im, flux_method=fm, n_case=0)
+    r.cons = c
+    ss = gpu_solver(2, [n, n], im=im, fm=fm, strict=True)
+    sf = gpu_solver(2, [n, n], im=im, fm=fm, strict=False)
+    ss.set_cons(c)
+    sf.set_cons(c)
+    for _ in range(10):
+        dt = r.max_dt()
+        assert ss.getTimeIntervalExplicit() == dt
+        r.solve(dt)
+        ss.solve(dt)
+        sf.solve(dt)
+    np.testing.assert_array_equal(ss.cons, r.cons)
+    if im in (2, 3, 15):  # continuous weights: differences stay at round-off
+        assert rel_linf(sf.cons, r.cons) < 1e-11
+    else:  # TENO cut-offs may flip on round-off near discontinuities: compare in L1
+        assert np.abs(sf.cons - r.cons).mean() / np.abs(r.cons).mean() < 1e-6
+
+
+@pytest.mark.parametrize("shape", [(5, 5), (7, 13), (100, 37), (33, 64)])
+def test_odd_sizes_and_segments_vs_reference(ref, shape):
+    rng = np.random.default_rng(sum(shape))
+    nx, ny = shape
+    c = quadrant_state((nx, ny), rng)
+    r = ref.RefSolver(2, [nx, ny], [0, 1, 0, 1, 0, 0], inter_method=2, flux_method=0, n_case=0)
+    r.cons = c
+    want = r.rhs()
+    for seg in ((0, 0, 0), (8, 8, 0), (64, 16, 0), (nx, ny, 0)):
+        s = gpu_solver(2, [nx, ny], [0, 1, 0, 1, 0, 0], strict=True, seg_len=seg)
+        s.set_cons(c)
+        np.testing.assert_array_equal(s.rhsSolve(), want, err_msg=str(seg))
+        s.close()
+
+
+def test_per_line_boundary_wiring_vs_reference(ref):
+    """Every boundary type, wired per line end as OneDBnd allows, against the reference."""
+    rng = np.random.default_rng(5)
+    nx, ny = 24, 20
+    c = quadrant_state((nx, ny), rng)
+    r = ref.RefSolver(2, [nx, ny], [0, 1, 0, 1, 0, 0], inter_method=11, flux_method=0, n_case=0)
+    r.cons = c
+    s = gpu_solver(2, [nx, ny], strict=True, im=11, fm=0)
+    s.set_cons(c)
+    kinds = ["outlet", "symx", "symy", "dir", "wrap", "mirror"]
+    for idim, nlines, n, stride in ((1, ny, nx, 1), (2, nx, ny, nx)):
+        for line in range(nlines):
+            base = line * (nx if idim == 1 else 1)
+            first, last = base, base + (n - 1) * stride
+            for side in (0, 1):
+                kind = kinds[rng.integers(len(kinds))]
+                vals = None
+                if kind == "outlet":
+                    typ, i0, off = 7, (first if side == 0 else last), 0
+                elif kind in ("symx", "symy"):
+                    typ = 10 if kind == "symx" else 11
+                    i0, off = (first, stride) if side == 0 else (last, -stride)
+                elif kind == "dir":
+                    typ, i0, off = 3, first, 0
+                    vals = np.column_stack([rng.uniform(0.5, 1.5, 4), rng.uniform(-1, 1, (4, 2)), rng.uniform(0.5, 1.5, 4)])
+                elif kind == "wrap":
+                    typ = 1
+                    i0, off = (last, -stride) if side == 0 else (first, stride)
+                else:
+                    typ = 1
+                    i0, off = (first, stride) if side == 0 else (last, -stride)
+                r.set_line_bc(idim, line, 0, side, typ, i0, off, vals)
+                s.set_line_bc(idim, line, 0, side, typ, i0, off, vals)
+    np.testing.assert_array_equal(s.rhsSolve(), r.rhs())
+    for _ in range(3):
+        dt = r.max_dt()
+        r.solve(dt)
+        s.solve(dt)
+    np.testing.assert_array_equal(s.cons, r.cons)
+
+
+# ----------------------------------------------------------------- 3D (oracle: the C restatement)
+@pytest.mark.parametrize("im,fm", [(2, 0), (11, 1), (8, 0)])
+def test_3d_against_c_oracle(im, fm):
+    from oracle.refsolver import ORC_WRAP, OracleC
+    rng = np.random.default_rng(im)
+    n = (12, 10, 14)
+    c = smooth_state_3d(n, rng)
+    zone_ = [0, 1.2, 0, 1, 0, 1]
+    h = gpu_solver(3, list(n), zone_, im=im, fm=fm).info.geth(0)
+    o = OracleC(3, list(n), h, im, fm, bc=[[ORC_WRAP] * 2] * 3)
+    o.cons = c
+    want = o.rhs()
+    for strict in (True, False):
+        s = gpu_solver(3, list(n), zone_, im=im, fm=fm, strict=strict, periodic=True)
+        s.set_cons(c)
+        got = s.rhsSolve()
+        if strict:
+            np.testing.assert_array_equal(got, want)
+        else:
+            assert rel_linf(got, want) < TOL_STEP
+        s.close()
+    s = gpu_solver(3, list(n), zone_, im=im, fm=fm, strict=True, periodic=True)
+    s.set_cons(c)
+    dt = o.max_dt(0.5)
+    assert s.getTimeIntervalExplicit() == dt
+    lo = o.solve(dt)
+    lg = s.solve(dt)
+    assert lo == lg
+    np.testing.assert_array_equal(s.cons, o.cons)
+
+
+def test_3d_outlet_and_symmetry_against_c_oracle():
+    from oracle.refsolver import ORC_OUTLET, ORC_SYMMETRY, OracleC
+    rng = np.random.default_rng(9)
+    n = (9, 11, 8)
+    c = smooth_state_3d(n, rng)
+    bc_o = [[ORC_OUTLET, ORC_SYMMETRY], [ORC_SYMMETRY, ORC_OUTLET], [ORC_SYMMETRY, ORC_SYMMETRY]]
+    bc_g = [[7, 10], [11, 7], [12, 12]]
+    s = gpu_solver(3, list(n), [0, 0.9, 0, 1, 0, 1], im=2, fm=0, strict=True, bc=bc_g)
+    o = OracleC(3, list(n), s.info.geth(0), 2, 0, bc=bc_o)
+    s.set_cons(c)
+    np.testing.assert_array_equal(s.rhsSolve(), o.rhs(c))
+
+
+@pytest.mark.parametrize("im,fm", [(2, 0), (11, 1)])
+def test_3d_z_invariant_reduces_to_2d_reference(ref, im, fm):
+    rng = np.random.default_rng(21)
+    n, nz = 16, 6
+    c2 = quadrant_state(n, rng)
+    r = ref.RefSolver(2, [n, n], [0, 1, 0, 1, 0, 0], inter_method=im, flux_method=fm, n_case=0, periodic=True)
+    r.cons = c2
+    p2 = r.prim
+    p3 = np.zeros((nz, n * n, 5))
+    p3[..., [0, 1, 2, 4]] = p2[None]
+    c3 = zone.prim_to_cons(p3.reshape(-1, 5))
+    s = gpu_solver(3, [n, n, nz], [0, 1, 0, 1, 0, 1], im=im, fm=fm, strict=True, periodic=True)
+    s.set_cons(c3)
+    got = s.rhsSolve().reshape(nz, n * n, 5)
+    # compare with the reference's rhs of the 2D state built from the same prim
+    r.cons = zone.prim_to_cons(p2)
+    want = r.rhs()
+    for k in range(nz):
+        assert rel_linf(got[k][:, [0, 1, 2, 4]], want) < 1e-12
+        assert np.abs(got[k][:, 3]).max() <= 1e-13 * np.abs(want).max()
+
+
+# ----------------------------------------------------------------- size-independent properties
+def test_periodic_conservation_full_size():
+    """Flux-difference form: totals of every conserved variable are invariant on a
+    periodic grid (2048^2, one RK3 step)."""
+    from tests.util import isentropic_vortex
+    c, h = isentropic_vortex(2048)
+    s = gpu_solver(2, [2048, 2048], [0, 10, 0, 10, 0, 0], im=11, fm=1, periodic=True, cfl=0.4)
+    s.set_cons(c)
+    tot0 = c.sum(0)
+    dt = s.getTimeIntervalExplicit()
+    s.solve(dt)
+    tot1 = s.cons.sum(0)
+    scale = np.abs(c).sum(0)
+    assert np.all(np.abs(tot1 - tot0) / scale < 1e-13)
+
+
+def test_nonfinite_state_reported():
+    n = 16
+    c = quadrant_state(n, np.random.default_rng(1))
+    c[37, 0] = np.nan
+    s = gpu_solver(2, [n, n])
+    s.set_cons(c)
+    with pytest.raises(_lib.CfdError) as e:
+        s.solve(1e-3)
+    assert e.value.code == -3
+
+
+# ----------------------------------------------------------------- device-resident loop (cfd_run)
+@pytest.mark.parametrize("strict", [True, False])
+def test_device_loop_sod_matches_reference(strict):
+    """cfd_run (dt, clipping and step control on the device, graph-captured
+    steps) reproduces the reference's stepsLoopCFL on Sod."""
+    g = np.load(GOLD / "sod_400.npz")
+    s = gpu_solver(1, [400], [-0.5, 0.5, 0, 0, 0, 0], im=2, fm=0, strict=strict)
+    s.set_cons(g["cons0"])
+    s.info.endStep = 1
+    s.info.outputDt = 0.2
+    dts, lin = s.run_device()
+    assert len(dts) == 349
+    if strict:
+        np.testing.assert_array_equal(dts, g["dts"])
+        np.testing.assert_array_equal(lin, g["linf"])
+        np.testing.assert_array_equal(s.cons, g["cons"])
+    else:
+        assert rel_linf(s.cons, g["cons"]) < TOL_RUN
+
+
+def test_device_loop_output_clipping_vs_reference(ref):
+    """Two output intervals with clipping on a 2D Riemann problem, against the
+    reference's loop; then a step-count-limited continuation."""
+    rng = np.random.default_rng(44)
+    n = 40
+    c = quadrant_state(n, rng)
+    r = ref.RefSolver(2, [n, n], [0, 1, 0, 1, 0, 0], inter_method=11, flux_method=0, n_case=0, cfl=0.5)
+    r.cons = c
+    rd, rl = r.run(2, 0.01)
+    s = gpu_solver(2, [n, n], im=11, fm=0, strict=True)
+    s.set_cons(c)
+    s.info.endStep = 2
+    s.info.outputDt = 0.01
+    dts, lin = s.run_device()
+    np.testing.assert_array_equal(dts, rd)
+    np.testing.assert_array_equal(lin, rl)
+    np.testing.assert_array_equal(s.cons, r.cons)
+    assert abs(s.info.t - r.t) == 0.0
+    # limited by max_steps: 7 steps (graphs of 3 + 3 + 1)
+    rd2, _ = r.run(10 ** 6, 1e9, 7)
+    s.info.step = 0
+    s.info.endStep = 10 ** 6
+    s.info.outputDt = 1e9
+    dts2, _ = s.run_device(max_steps=7)
+    np.testing.assert_array_equal(dts2, rd2)
+    np.testing.assert_array_equal(s.cons, r.cons)
