@@ -122,11 +122,24 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- reference arm
+def usable_cores() -> int:
+    """Cores this process may run on: the affinity mask, capped by a cgroup CPU
+    quota (OpenMP oversubscription of a quota makes the reference crawl)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        q = Path("/sys/fs/cgroup/cpu.max").read_text().split()
+        if q[0] != "max":
+            n = min(n, max(1, int(float(q[0]) / float(q[1]))))
+    except Exception:
+        pass
+    return max(1, n)
+
+
 def reference_throughput(dim, n, L, im, fm, cfl, budget_s=12.0, max_steps=50):
     """The reference zone_FD CPU solver (oracle/_ref/libcongfd_ref.so, compiled
     from its own sources) on the same workload; OpenMP over all host cores."""
     from oracle.refsolver import OracleC, RefSolver, ORC_WRAP
-    threads = os.cpu_count() or 1
+    threads = usable_cores()
     c, h = initial_state(dim, n, L)
     if dim == 2:
         kind = "reference"
@@ -152,7 +165,7 @@ def reference_throughput(dim, n, L, im, fm, cfl, budget_s=12.0, max_steps=50):
     ncell = n ** dim
     return {"value": ncell * k / el, "unit": "cell-steps/s", "cores": threads, "kind": kind,
             "sample": f"{k} timed RK3 steps (after 1 warm-up step of {warm:.1f} s) of the full {n}^{dim} grid, "
-                      f"{el:.1f} s, OpenMP threads = {threads}"}
+                      f"{el:.1f} s, OpenMP threads = {threads} (os.cpu_count() = {os.cpu_count()})"}
 
 
 # --------------------------------------------------------------------- our arm
@@ -312,7 +325,7 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=150)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="vortex2048", choices=sorted(WORKLOADS))
