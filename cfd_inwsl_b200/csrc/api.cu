@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) wave_speed_kernel(const double *__restric
 // Step control of stepsLoopCFL (blockSolver.cpp:176-201) on the device: the
 // loop test, dt = CFL / sum_d lambda_d from the wave-speed maxima of the
 // current state, clipping to the output interval, stage coefficients.
-__global__ void step_begin_kernel(cfd::StepCtl *c, const unsigned long long *red, int dim, double *dts)
+__global__ void step_begin_kernel(cfd::StepCtl *c, unsigned long long *red, int dim, double *dts)
 {
     if (c->done) return;
     if (!(c->step < c->endStep && c->k < c->maxSteps)) {
@@ -101,6 +101,9 @@ __global__ void step_begin_kernel(cfd::StepCtl *c, const unsigned long long *red
     c->tst[2] = c->t + dt;
     c->tst[3] = c->tst[2] - dt / 2;
     if (dts) dts[c->k] = dt;
+    // the wave speeds are consumed: clear the reduction words for this step's
+    // third stage (only when the step runs, so a finished loop keeps them)
+    for (int i = 0; i < 4; i++) red[i] = 0ULL;
 }
 
 // BlockSolver::solve's time update and the per-step log value (rhoLinf).
@@ -503,7 +506,6 @@ int enqueue_step(cfd_handle *h, int cur)
     int rc;
     if ((rc = rk_stage(h, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl))) return rc;
     if ((rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl))) return rc;
-    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
     if ((rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl))) return rc;
     step_end_kernel<<<1, 1, 0, h->stream>>>(h->ctl, h->red, h->d_linf);
     CFD_CUDA(h, cudaGetLastError());
@@ -933,3 +935,4 @@ int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr
 }
 
 } // extern "C"
+
