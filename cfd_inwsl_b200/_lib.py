@@ -78,6 +78,7 @@ _PROTOS = {
     "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_launch_count": (C.c_ulonglong, [C.c_void_p]),
     "cfd_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double]),
+    "cfd_rhs_noalloc": (C.c_int, [C.POINTER(CfdConfig), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 }
 
 

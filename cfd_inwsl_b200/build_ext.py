@@ -51,6 +51,8 @@ def units() -> list[tuple[Path, Path, list[str]]]:
                 out.append((CSRC / "sweep_inst.cu", obj, flags, headers))
     out.append((CSRC / "api.cu", BUILD / "api.o", ["--fmad=false", "-DCFD_NS=api"],
                 headers + [CSRC / "sweep_dispatch.h", ROOT / "include" / "cfdgpu.h"]))
+    out.append((CSRC / "noalloc.cu", BUILD / "noalloc.o", ["--fmad=false", "-DCFD_NS=api"],
+                headers + [CSRC / "sweep_dispatch.h", ROOT / "include" / "cfdgpu.h"]))
     return out
 
 

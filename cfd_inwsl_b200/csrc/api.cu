@@ -936,3 +936,14 @@ int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr
 
 } // extern "C"
 
+// Selector lookup shared with the allocation-free entry point (noalloc.cu).
+namespace cfd {
+bool map_inter_method_for(int inter_method, int dim, int *fam, double *c)
+{
+    InterMap im = map_inter_method(inter_method, dim);
+    if (!im.ok) return false;
+    *fam = im.fam;
+    *c = im.c;
+    return true;
+}
+} // namespace cfd

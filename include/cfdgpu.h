@@ -168,6 +168,31 @@ int cfd_sweep(cfd_handle *h, int idim, int mode, double t);
 int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double *out);
 int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr, int n, double *out);
 
+/* Allocation-free RHS evaluation (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory: code that runs inside
+ * another framework's memory pool, or a program that reserved all device
+ * memory before loading this library. It takes the caller's device buffers,
+ * cons_soa (input state) and rhs_soa (output), both planar SoA
+ * [var * ncell + cell] with ncell = n[0]*n[1]*n[2], evaluates one RHS exactly
+ * as cfd_rhs does for the same cfg (default boundary wiring from cfg->bc), and
+ * enqueues everything on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) without synchronising. It calls no cudaMalloc/cudaFree and no
+ * allocating library routine.
+ *
+ * Its only scratch, the ghost wiring of every line end, lives in a file-scope
+ * device array of CFD_NOALLOC_MAX_LINE_ENDS entries (768 KiB) that each GPU
+ * loading the library holds until the process exits. Grids with more line
+ * ends than that (sum over directions of 2 * ncell / n[d]; 2D grids up to
+ * 4096 x 4096 fit) are rejected with CFD_ERR_CONFIG and a message on stderr.
+ * The first call on a device looks up the array's device address (once per
+ * device, with cfg->device made current); make that first call before any
+ * stream capture. Every call rewrites the part of the array it uses, and all
+ * calls share it: calls that overlap on the GPU (different streams, or other
+ * threads) race on the array and must be serialised by the caller. */
+#define CFD_NOALLOC_MAX_LINE_ENDS 16384
+int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, double *rhs_soa, double t, void *stream);
+
 /* Library version string. */
 const char *cfd_version(void);
 
