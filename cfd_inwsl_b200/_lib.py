@@ -75,6 +75,7 @@ _PROTOS = {
     "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_version": (C.c_char_p, []),
+    "cfd_eval_face": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_launch_count": (C.c_ulonglong, [C.c_void_p]),
     "cfd_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double]),
@@ -134,4 +135,13 @@ def eval_flux(dim: int, ax: int, flux_method: int, lr: np.ndarray, strict: bool 
     n = lr.shape[0]
     out = np.empty((n, nv))
     check(load().cfd_eval_flux(dim, ax, flux_method, int(strict), ptr(lr), n, ptr(out)))
+    return out
+
+
+def eval_face(dim: int, ax: int, inter_method: int, prims6: np.ndarray, precision: int = 0) -> np.ndarray:
+    """Device face reconstruction of n six-cell stencils (n x 6 x nvar prims) -> n x 2*nvar."""
+    prims6 = np.ascontiguousarray(prims6, dtype=np.float64)
+    n = prims6.shape[0]
+    out = np.empty((n, 2 * (dim + 2)))
+    check(load().cfd_eval_face(dim, ax, inter_method, precision, ptr(prims6), n, ptr(out)))
     return out

@@ -41,7 +41,7 @@ def common_flags() -> list[str]:
 
 def units() -> list[tuple[Path, Path, list[str]]]:
     out = []
-    headers = [CSRC / f for f in ("euler_math.cuh", "sweep.cuh", "sweep_params.h")]
+    headers = [CSRC / f for f in ("euler_math.cuh", "mixed.cuh", "sweep.cuh", "sweep_params.h")]
     for flavour in ("strict", "fast"):
         for nv in NVS:
             for fam in FAMILIES:

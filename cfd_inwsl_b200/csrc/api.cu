@@ -10,6 +10,7 @@
 // reference's arithmetic bit for bit.
 #include "cfdgpu.h"
 #include "euler_math.cuh"
+#include "mixed.cuh"
 #include "sweep_dispatch.h"
 
 #include <cmath>
@@ -136,6 +137,32 @@ __global__ void eval_flux_kernel(const double *lr, int n, double *out)
         }
         cfd::riemann<NV, AX, FLUX>(L, R, f);
         for (int v = 0; v < NV; v++) out[NV * i + v] = f[v];
+    }
+}
+
+// One face reconstruction per thread from six stencil prims (known-answer hook).
+template <int NV, int AX, int FAM, int PREC>
+__global__ void eval_face_kernel(const double *prims6, int n, double c, double *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double pr6[6][NV], cs6[6][NV];
+    for (int j = 0; j < 6; j++) {
+        for (int v = 0; v < NV; v++) pr6[j][v] = prims6[(i * 6 + j) * NV + v];
+        cfd::prim_to_cons<NV>(pr6[j], cs6[j]);
+    }
+    double fl[NV], fr[NV];
+    if constexpr (NV == 3) {
+        cfd::reconstruct_face<NV, AX, FAM>(pr6, cs6, c, fl, fr);
+    } else {
+        auto cs = [&](int j, int v) { return cs6[j][v]; };
+        auto pr = [&](int j, int v) { return pr6[j][v]; };
+        if constexpr (PREC == 1) cfd::reconstruct_face_mixed<NV, AX, FAM>(cs, pr, c, fl, fr);
+        else cfd::reconstruct_face_stream<NV, AX, FAM>(cs, pr, c, fl, fr);
+    }
+    for (int v = 0; v < NV; v++) {
+        out[i * 2 * NV + v] = fl[v];
+        out[i * 2 * NV + NV + v] = fr[v];
     }
 }
 
@@ -376,6 +403,7 @@ SweepParams base_params(cfd_handle *h, int d)
     p.bc_vals = h->d_bcvals;
     p.icst = h->icst;
     p.seg_len = h->seg_len[d];
+    p.prec = h->cfg.precision == CFD_PREC_MIXED ? 1 : 0;
     p.dm_u = h->dm_u;
     p.dm_v = h->dm_v;
     return p;
@@ -566,7 +594,10 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     if (cfg->gamma != 1.4) return CFD_ERR_UNSUPPORTED;
     if (cfg->diff_method != CFD_DIFF_MND6) return CFD_ERR_UNSUPPORTED;
     if (cfg->flux_method != CFD_FLUX_HLLC && cfg->flux_method != CFD_FLUX_ROE) return CFD_ERR_CONFIG;
-    if (cfg->precision != CFD_PREC_FP64) return CFD_ERR_UNSUPPORTED;
+    if (cfg->precision != CFD_PREC_FP64 && cfg->precision != CFD_PREC_MIXED) return CFD_ERR_CONFIG;
+    // the mixed form reconstructs in FP32 (multi-dimensional fast flavour only);
+    // the strict flavour is the bit-for-bit FP64 build
+    if (cfg->precision == CFD_PREC_MIXED && (cfg->dim < 2 || cfg->strict)) return CFD_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) {
         if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
         if (d >= cfg->dim && cfg->n[d] != 1) return CFD_ERR_CONFIG;
@@ -935,6 +966,41 @@ int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr
 }
 
 } // extern "C"
+
+extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, const double *prims6, int n,
+                             double *out)
+{
+    if (dim < 1 || dim > 3 || ax < 0 || ax >= dim || (precision != 0 && precision != 1)) return CFD_ERR_CONFIG;
+    if (precision == 1 && dim == 1) return CFD_ERR_UNSUPPORTED;
+    InterMap im = map_inter_method(inter_method, dim);
+    if (!im.ok) return CFD_ERR_UNSUPPORTED;
+    if (n <= 0) return CFD_OK;
+    int nv = dim + 2;
+    double *din = nullptr, *dout = nullptr;
+    if (cudaMalloc(&din, sizeof(double) * 6 * nv * n) != cudaSuccess) return CFD_ERR_NOMEM;
+    if (cudaMalloc(&dout, sizeof(double) * 2 * nv * n) != cudaSuccess) {
+        cudaFree(din);
+        return CFD_ERR_NOMEM;
+    }
+    cudaMemcpy(din, prims6, sizeof(double) * 6 * nv * n, cudaMemcpyHostToDevice);
+    int g = (n + 127) / 128;
+    bool launched = false;
+#define CFD_EFACE(NV, AX, F)                                                                                  \
+    if (!launched && nv == NV && ax == AX && im.fam == F) {                                                   \
+        if (precision == 1) eval_face_kernel<NV, AX, F, (NV >= 4 ? 1 : 0)><<<g, 128>>>(din, n, im.c, dout);  \
+        else eval_face_kernel<NV, AX, F, 0><<<g, 128>>>(din, n, im.c, dout);                                  \
+        launched = true;                                                                                      \
+    }
+#define CFD_EFACE_F(F) CFD_EFACE(3, 0, F) CFD_EFACE(4, 0, F) CFD_EFACE(4, 1, F) CFD_EFACE(5, 0, F) \
+                       CFD_EFACE(5, 1, F) CFD_EFACE(5, 2, F)
+    CFD_EFACE_F(0) CFD_EFACE_F(1) CFD_EFACE_F(2) CFD_EFACE_F(3) CFD_EFACE_F(4)
+#undef CFD_EFACE_F
+#undef CFD_EFACE
+    cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * 2 * nv * n, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(dout);
+    return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
+}
 
 // Selector lookup shared with the allocation-free entry point (noalloc.cu).
 namespace cfd {

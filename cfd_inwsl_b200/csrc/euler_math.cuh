@@ -23,6 +23,13 @@ namespace cfd {
 // zone_FD/src/include/macro.hpp:28 (#define GAMMA 1.4)
 constexpr double kGamma = 1.4;
 
+#if defined(CFD_FAST)
+// fast path: reciprocals shared across a state or a face, multiplications
+// instead of repeated IEEE divisions (about 1 ulp from the reference's order).
+constexpr double kG1 = kGamma / (kGamma - 1);   // gamma / (gamma - 1)
+constexpr double kInvGm1 = 1.0 / (kGamma - 1);  // 1 / (gamma - 1)
+#endif
+
 // ---------------------------------------------------------------------------
 // Five-point interpolators (zone_FD/src/include/interScheme.hpp).
 // q0..q4 are the five upwind-ordered point values; the result is the value at
@@ -130,9 +137,26 @@ CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, doub
         double b0, b1, b2;
         smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
         double tau = fabs(b2 - b0), t;
+#if defined(CFD_FAST)
+        // fast path: tau/s_k from one reciprocal of s0 s1 s2 (guarded against
+        // overflow/underflow of the product)
+        const double s0 = b0 + eps, s1 = b1 + eps, s2 = b2 + eps;
+        const double s01 = s0 * s1, prod = s01 * s2;
+        double r0, r1, r2;
+        if (prod > 1e-280 && prod < 1e280) {
+            const double ti = tau / prod;
+            r0 = ti * (s1 * s2); r1 = ti * (s0 * s2); r2 = ti * s01;
+        } else {
+            r0 = tau / s0; r1 = tau / s1; r2 = tau / s2;
+        }
+        t = 1.0 + r0; t *= t; b0 = t * t * t;
+        t = 1.0 + r1; t *= t; b1 = t * t * t;
+        t = 1.0 + r2; t *= t; b2 = t * t * t;
+#else
         t = 1.0 + tau / (b0 + eps); t *= t; b0 = t * t * t;
         t = 1.0 + tau / (b1 + eps); t *= t; b1 = t * t * t;
         t = 1.0 + tau / (b2 + eps); t *= t; b2 = t * t * t;
+#endif
         double sumbeta = 0.0;
         sumbeta += b0; sumbeta += b1; sumbeta += b2;
         double CT = c * sumbeta;
@@ -185,21 +209,37 @@ CFD_HD void cons_to_prim(const double *c, double *p)
     const double gamma = kGamma;
     if constexpr (NV == 3) {
         double r = c[0], ru = c[1], rE = c[2];
+#if defined(CFD_FAST)
+        const double ir = 1.0 / r;
+        double u = ru * ir;
+        double E = rE * ir;
+#else
         double u = ru / r;
         double E = rE / r;
+#endif
         double e = -u * u / 2 + E;
         double RT = (gamma - 1) * e;
         p[0] = r; p[1] = u; p[2] = r * RT;
     } else if constexpr (NV == 4) {
         double r = c[0], ru = c[1], rv = c[2], rE = c[3];
+#if defined(CFD_FAST)
+        const double ir = 1.0 / r;
+        double u = ru * ir, v = rv * ir, E = rE * ir;
+#else
         double u = ru / r, v = rv / r, E = rE / r;
+#endif
         double q2 = (u * u + v * v) / 2;
         double e = -q2 + E;
         double RT = (gamma - 1) * e;
         p[0] = r; p[1] = u; p[2] = v; p[3] = r * RT;
     } else {
         double r = c[0], ru = c[1], rv = c[2], rw = c[3], rE = c[4];
+#if defined(CFD_FAST)
+        const double ir = 1.0 / r;
+        double u = ru * ir, v = rv * ir, w = rw * ir, E = rE * ir;
+#else
         double u = ru / r, v = rv / r, w = rw / r, E = rE / r;
+#endif
         double q2 = (u * u + v * v + w * w) / 2;
         double e = -q2 + E;
         double RT = (gamma - 1) * e;
@@ -216,15 +256,27 @@ CFD_HD void prim_to_cons(const double *p, double *c)
     if constexpr (NV == 3) {
         double rt = p[0], ut = p[1], pt = p[2];
         double ekt = (ut * ut) / 2;
+#if defined(CFD_FAST)
+        c[0] = rt; c[1] = rt * ut; c[2] = pt * kInvGm1 + rt * ekt;
+#else
         c[0] = rt; c[1] = rt * ut; c[2] = pt / (gamma - 1) + rt * ekt;
+#endif
     } else if constexpr (NV == 4) {
         double rt = p[0], ut = p[1], vt = p[2], pt = p[3];
         double ekt = (ut * ut + vt * vt) / 2;
+#if defined(CFD_FAST)
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = pt * kInvGm1 + rt * ekt;
+#else
         c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = pt / (gamma - 1) + rt * ekt;
+#endif
     } else {
         double rt = p[0], ut = p[1], vt = p[2], wt = p[3], pt = p[4];
         double ekt = (ut * ut + vt * vt + wt * wt) / 2;
+#if defined(CFD_FAST)
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = pt * kInvGm1 + rt * ekt;
+#else
         c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = pt / (gamma - 1) + rt * ekt;
+#endif
     }
 }
 
@@ -247,8 +299,13 @@ struct Eigen {
         if constexpr (NV == 3) {
             double rl = pl[0], ul = pl[1], pL = pl[2];
             double rr = pr[0], ur = pr[1], pR = pr[2];
+#if defined(CFD_FAST)
+            double HL = 0.5 * (ul * ul) + pL * (kG1 / rl);
+            double HR = 0.5 * (ur * ur) + pR * (kG1 / rr);
+#else
             double HL = (ul * ul) / 2 + pL / rl * gamma / (gamma - 1);
             double HR = (ur * ur) / 2 + pR / rr * gamma / (gamma - 1);
+#endif
             double coef1 = sqrt(rl), coef2 = sqrt(rr);
             double divisor = 1.0 / (coef1 + coef2);
             double u = (coef1 * ul + coef2 * ur) * divisor;
@@ -270,6 +327,14 @@ struct Eigen {
             double vr[3] = {pr[1], pr[2], D == 3 ? pr[3] : 0.0};
             double rl = pl[0], rr = pr[0], pL = pl[NV - 1], pR = pr[NV - 1];
             double HL, HR;
+#if defined(CFD_FAST)
+            {
+                double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+                if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+                HL = 0.5 * kl + pL * (kG1 / rl);
+                HR = 0.5 * kr + pR * (kG1 / rr);
+            }
+#else
             if constexpr (D == 2) {
                 HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pL / rl * gamma / (gamma - 1);
                 HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pR / rr * gamma / (gamma - 1);
@@ -277,6 +342,7 @@ struct Eigen {
                 HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pL / rl * gamma / (gamma - 1);
                 HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pR / rr * gamma / (gamma - 1);
             }
+#endif
             double coef1 = sqrt(rl), coef2 = sqrt(rr);
             double divisor = 1.0 / (coef1 + coef2);
             double u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
@@ -321,12 +387,16 @@ struct Eigen {
             L[2][1] = (CFD_DIV_C(-nx) - CFD_DIV_H(u)) / 2;
             L[2][2] = (CFD_DIV_C(-ny) - CFD_DIV_H(v)) / 2;
             if constexpr (D == 3) L[2][3] = (CFD_DIV_C(-nz) - CFD_DIV_H(w)) / 2;
+#if defined(CFD_FAST)
+            L[2][E] = 0.5 * ih;
+#else
             L[2][E] = 1.0 / (2.0 * h);
+#endif
             L[3][0] = (CFD_DIV_C(-Vn) + CFD_DIV_H(ek)) / 2;
             L[3][1] = (CFD_DIV_C(nx) - CFD_DIV_H(u)) / 2;
             L[3][2] = (CFD_DIV_C(ny) - CFD_DIV_H(v)) / 2;
             if constexpr (D == 3) L[3][3] = (CFD_DIV_C(nz) - CFD_DIV_H(w)) / 2;
-            L[3][E] = 1.0 / (2.0 * h);
+            L[3][E] = L[2][E];
             if constexpr (D == 3) {
                 if constexpr (AX != 2) {
                     L[4][0] = -w; L[4][1] = 0.0; L[4][2] = 0.0; L[4][3] = 1.0; L[4][4] = 0.0;
@@ -341,7 +411,7 @@ struct Eigen {
             } else {
                 R[0][0] = 0; R[1][0] = 1.0; R[2][0] = 0.0; R[3][0] = 0.0; R[E][0] = u;
             }
-            R[0][1] = 1.0 / h; R[1][1] = CFD_DIV_H(u); R[2][1] = CFD_DIV_H(v); R[E][1] = CFD_DIV_H(ek);
+            R[0][1] = CFD_DIV_H(1.0); R[1][1] = CFD_DIV_H(u); R[2][1] = CFD_DIV_H(v); R[E][1] = CFD_DIV_H(ek);
             if constexpr (D == 3) R[3][1] = CFD_DIV_H(w);
             R[0][2] = 1; R[1][2] = u - nx * c; R[2][2] = v - ny * c; R[E][2] = h + ek - Vn * c;
             if constexpr (D == 3) R[3][2] = w - nz * c;
@@ -401,17 +471,29 @@ CFD_HD void char_cons_to_prim(const double *cs, double *p)
         // eigensystemEuler1D::consToPrim (eigenSystem.cpp:309-322)
         double rt = cs[0], rut = cs[1], ret = cs[2];
         double ut = rut / rt;
-        double ekt = (ut * ut) / 2;
+        double ekt = (ut * ut) / 2;  // one division only
         p[0] = rt; p[1] = ut; p[2] = (gamma - 1) * (ret - rt * ekt);
     } else if constexpr (NV == 4) {
         double rt = cs[0], rut = cs[1], rvt = cs[2], ret = cs[3];
+#if defined(CFD_FAST)
+        const double irt = 1.0 / rt;
+        double ut = rut * irt, vt = rvt * irt;
+        double rekt = (rut * rut + rvt * rvt) * (0.5 * irt);
+#else
         double ut = rut / rt, vt = rvt / rt;
         double rekt = (rut * rut + rvt * rvt) / rt / 2;
+#endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = (gamma - 1) * (ret - rekt);
     } else {
         double rt = cs[0], rut = cs[1], rvt = cs[2], rwt = cs[3], ret = cs[4];
+#if defined(CFD_FAST)
+        const double irt = 1.0 / rt;
+        double ut = rut * irt, vt = rvt * irt, wt = rwt * irt;
+        double rekt = (rut * rut + rvt * rvt + rwt * rwt) * (0.5 * irt);
+#else
         double ut = rut / rt, vt = rvt / rt, wt = rwt / rt;
         double rekt = (rut * rut + rvt * rvt + rwt * rwt) / rt / 2;
+#endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = wt; p[4] = (gamma - 1) * (ret - rekt);
     }
 }
@@ -485,6 +567,195 @@ CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], d
             for (int i = 1; i < NV - 1; i++) fr[i] = pr6[2][i];
             fr[NV - 1] = pr6[3][NV - 1];
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Streaming form of the multi-dimensional reconstruction (NV = 4, 5): the Roe
+// average is kept as a handful of scalars, eigenvector entries are formed when
+// a characteristic field needs them, stencil values are read through an
+// accessor (shared memory in the sweep), and the fields are processed in the
+// reference's back-projection order 2, 3, 1, 0 (then 4), so each face state
+// component accumulates with exactly the rounding of eigenSystem.cpp:139-149.
+// Far fewer values are live at once than with the full 4x4 / 5x5 matrices.
+// ---------------------------------------------------------------------------
+template <int NV, int AX>
+struct EigenBase {
+    double u, v, w, h, c, ek, Vn;
+#if defined(CFD_FAST)
+    double ic, ih;
+#endif
+    static constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0, nz = (AX == 2) ? 1.0 : 0.0;
+
+    // the same base quantities as Eigen<NV,AX>'s constructor (eigenSystem.cpp:13-52)
+    template <class PR>
+    CFD_HD EigenBase(const PR &pr)
+    {
+        constexpr int D = NV - 2;
+        const double gamma = kGamma;
+        double vl[3] = {pr(2, 1), pr(2, 2), D == 3 ? pr(2, 3) : 0.0};
+        double vr[3] = {pr(3, 1), pr(3, 2), D == 3 ? pr(3, 3) : 0.0};
+        double rl = pr(2, 0), rr = pr(3, 0), pL = pr(2, NV - 1), pR = pr(3, NV - 1);
+        double HL, HR;
+#if defined(CFD_FAST)
+        {
+            double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+            if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+            HL = 0.5 * kl + pL * (kG1 / rl);
+            HR = 0.5 * kr + pR * (kG1 / rr);
+        }
+#else
+        if constexpr (D == 2) {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pL / rl * gamma / (gamma - 1);
+            HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pR / rr * gamma / (gamma - 1);
+        } else {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pL / rl * gamma / (gamma - 1);
+            HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pR / rr * gamma / (gamma - 1);
+        }
+#endif
+        double coef1 = sqrt(rl), coef2 = sqrt(rr);
+        double divisor = 1.0 / (coef1 + coef2);
+        u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
+        v = (coef1 * vl[1] + coef2 * vr[1]) * divisor;
+        w = (D == 3) ? (coef1 * vl[2] + coef2 * vr[2]) * divisor : 0.0;
+        double ht = (coef1 * HL + coef2 * HR) * divisor;
+        if constexpr (D == 2) {
+            Vn = nx * u + ny * v;
+            ek = (u * u + v * v) / 2;
+        } else {
+            Vn = nx * u + ny * v + nz * w;
+            ek = (u * u + v * v + w * w) / 2;
+        }
+        h = ht - ek;
+        c = sqrt((gamma - 1) * h);
+#if defined(CFD_FAST)
+        ic = 1.0 / c;
+        ih = 1.0 / h;
+#endif
+    }
+#if defined(CFD_FAST)
+    CFD_HD double dc(double a) const { return a * ic; }
+    CFD_HD double dh(double a) const { return a * ih; }
+#else
+    CFD_HD double dc(double a) const { return a / c; }
+    CFD_HD double dh(double a) const { return a / h; }
+#endif
+    // left eigenvector k, column m (eigenSystem.cpp:53-68 and the 3D extension)
+    CFD_HD double L(int k, int m) const
+    {
+        constexpr int E = NV - 1;
+        if (k == 0) {
+            if (AX != 2) return m == 0 ? (-ny * u + nx * v) : m == 1 ? ny : m == 2 ? (-nx) : (m == E ? 0 : 0.0);
+            return m == 0 ? -u : m == 1 ? 1.0 : 0.0;
+        }
+        if (k == 1) return m == 0 ? (h - ek) : m == 1 ? u : m == 2 ? v : m == E ? -1.0 : w;
+        if (k == 2 || k == 3) {
+            const double s = (k == 2) ? -1.0 : 1.0;
+            if (m == E) {
+#if defined(CFD_FAST)
+                return 0.5 * ih;
+#else
+                return 1.0 / (2.0 * h);
+#endif
+            }
+            if (m == 0) return (k == 2) ? (dc(Vn) + dh(ek)) / 2 : (dc(-Vn) + dh(ek)) / 2;
+            if (m == 1) return (dc(s * nx) - dh(u)) / 2;
+            if (m == 2) return (dc(s * ny) - dh(v)) / 2;
+            return (dc(s * nz) - dh(w)) / 2;
+        }
+        // k == 4: second shear wave (3D only)
+        if (AX != 2) return m == 0 ? -w : m == 3 ? 1.0 : 0.0;
+        return m == 0 ? -v : m == 2 ? 1.0 : 0.0;
+    }
+    // right eigenvector k, row i (eigenSystem.cpp:70-85 and the 3D extension)
+    CFD_HD double R(int i, int k) const
+    {
+        constexpr int E = NV - 1;
+        if (k == 0) {
+            if (AX != 2) return i == 0 ? 0.0 : i == 1 ? ny : i == 2 ? -nx : i == E ? ny * u - nx * v : 0.0;
+            return i == 1 ? 1.0 : i == E ? u : 0.0;
+        }
+        if (k == 1) return i == 0 ? dh(1.0) : i == 1 ? dh(u) : i == 2 ? dh(v) : i == E ? dh(ek) : dh(w);
+        if (k == 2 || k == 3) {
+            const double s = (k == 2) ? -1.0 : 1.0;
+            if (i == 0) return 1.0;
+            if (i == E) return (k == 2) ? h + ek - Vn * c : h + ek + Vn * c;
+            if (i == 1) return (k == 2) ? u - nx * c : u + nx * c;
+            if (i == 2) return (k == 2) ? v - ny * c : v + ny * c;
+            (void)s;
+            return (k == 2) ? w - nz * c : w + nz * c;
+        }
+        if (AX != 2) return i == 3 ? 1.0 : i == 4 ? w : 0.0;
+        return i == 2 ? 1.0 : i == 4 ? v : 0.0;
+    }
+};
+
+// cs(j, v): re-derived cons of stencil cell j (0..5), pr(j, v): its prim.
+template <int NV, int AX, int FAM, class CS, class PR>
+CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, double *fl, double *fr)
+{
+    static_assert(NV == 4 || NV == 5, "multi-dimensional form");
+    const EigenBase<NV, AX> eb(pr);
+    double cl[NV], cr[NV];
+    // Fully unrolled: the instruction-level parallelism across fields beats the
+    // smaller code of a rolled loop (measured on B200: 22.0 vs 31.9 ms per 3D
+    // 256^3 step). CFD_ROLL_FIELDS builds the rolled form (uniform branches).
+#if defined(CFD_ROLL_FIELDS)
+#pragma unroll 1
+#else
+#pragma unroll
+#endif
+    for (int kk = 0; kk < NV; kk++) {
+        const int k = (kk == 0) ? 2 : (kk == 1) ? 3 : (kk == 2) ? 1 : (kk == 3) ? 0 : 4;
+        double l[NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
+        double q[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            // primToChar's order: rut L1 + rvt L2 [+ rwt L3] + ret LE + rt L0
+            double a = cs(j, 1) * l[1] + cs(j, 2) * l[2];
+#pragma unroll
+            for (int m = 3; m < NV; m++) a = a + cs(j, m) * l[m];
+            q[j] = a + cs(j, 0) * l[0];
+        }
+        double QL, QR;
+#if !defined(CFD_ROLL_FIELDS)
+        QL = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst);
+        QR = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst);
+#else
+        // one interpolator body for both states (mirrored stencil on side 1)
+#pragma unroll 1
+        for (int side = 0; side < 2; side++) {
+            const bool m = side != 0;
+            const double r = inter5<FAM>(m ? q[5] : q[0], m ? q[4] : q[1], q[m ? 3 : 2], q[m ? 2 : 3],
+                                         m ? q[1] : q[4], icst);
+            if (m) QR = r; else QL = r;
+        }
+#endif
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            const double r = eb.R(i, k);
+            if (kk == 0) {
+                cl[i] = QL * r;
+                cr[i] = QR * r;
+            } else {
+                cl[i] = cl[i] + QL * r;
+                cr[i] = cr[i] + QR * r;
+            }
+        }
+    }
+    char_cons_to_prim<NV>(cl, fl);
+    char_cons_to_prim<NV>(cr, fr);
+    // crude positivity fallback (reconstructor5order.hpp:380-381), including
+    // the reference's mix of right density/pressure with left velocity.
+    if (fl[0] < 0 || fl[NV - 1] < 0) {
+        for (int i = 0; i < NV; i++) fl[i] = pr(2, i);
+    }
+    if (fr[0] < 0 || fr[NV - 1] < 0) {
+        fr[0] = pr(3, 0);
+        for (int i = 1; i < NV - 1; i++) fr[i] = pr(2, i);
+        fr[NV - 1] = pr(3, NV - 1);
     }
 }
 
@@ -567,6 +838,17 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
     double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
     const double *vl = L + 1, *vr = R + 1;
     double HL, HR;
+#if defined(CFD_FAST)
+    const double prl = pl * (1.0 / rl), prr = pr * (1.0 / rr);  // p / rho
+    {
+        double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+        if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+        HL = 0.5 * kl + prl * kG1;
+        HR = 0.5 * kr + prr * kG1;
+    }
+    double VnL = vl[AX], VnR = vr[AX];
+    double cl = sqrt(prl * gamma), cr = sqrt(prr * gamma);
+#else
     if constexpr (D == 2) {
         HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
         HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
@@ -576,6 +858,7 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
     }
     double VnL = vl[AX], VnR = vr[AX];
     double cl = sqrt(pl / rl * gamma), cr = sqrt(pr / rr * gamma);
+#endif
     double rBar = (rl + rr) / 2, cBar = (cl + cr) / 2;
     double ps0 = (pl + pr) / 2 - rBar * cBar * (VnR - VnL) / 2;
     double ps = (0.0 < ps0) ? ps0 : 0.0;  // std::max(0.0, .)
@@ -634,6 +917,14 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
     const double *vl = L + 1, *vr = R + 1;
     double HL, HR;
+#if defined(CFD_FAST)
+    {
+        double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+        if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+        HL = 0.5 * kl + pl * (kG1 / rl);
+        HR = 0.5 * kr + pr * (kG1 / rr);
+    }
+#else
     if constexpr (D == 2) {
         HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
         HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
@@ -641,6 +932,7 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
         HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
         HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
     }
+#endif
     double VnL = vl[AX], VnR = vr[AX];
     double FcL[NV], FcR[NV];
     FcL[0] = rl * VnL;
@@ -663,24 +955,45 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double VnAvg = vAvg[AX];
     double lambda[3] = {fabs(VnAvg - cAvg), fabs(VnAvg), fabs(VnAvg + cAvg)};
     double eps = 0.05 * (fabs(VnAvg) + cAvg);
+#if defined(CFD_FAST)
+    {
+        const double ie2 = 0.5 / eps;
+        for (int i = 0; i < 3; i++)
+            if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) * ie2;
+    }
+    const double ic2 = 1.0 / (cAvg * cAvg);
+#else
     for (int i = 0; i < 3; i++)
         if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) / (2.0 * eps);
+#endif
 
     double deltaP = pr - pl, deltaVn = VnR - VnL, deltaRho = rr - rl;
     double dv[3];
     for (int i = 0; i < D; i++) dv[i] = vr[i] - vl[i];
     double Fd[NV];
+#if defined(CFD_FAST)
+    double c1 = (deltaP - rhoAvg * cAvg * deltaVn) * (0.5 * ic2);
+#else
     double c1 = (deltaP - rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+#endif
     Fd[0] = lambda[0] * (c1 * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] = lambda[0] * (c1 * (vAvg[i] - cAvg * n[i]));
     Fd[E] = lambda[0] * (c1 * (HAvg - cAvg * VnAvg));
 
+#if defined(CFD_FAST)
+    double cc = (deltaP + rhoAvg * cAvg * deltaVn) * (0.5 * ic2);
+#else
     double cc = (deltaP + rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+#endif
     Fd[0] += lambda[2] * (cc * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] += lambda[2] * (cc * (vAvg[i] + cAvg * n[i]));
     Fd[E] += lambda[2] * (cc * (HAvg + cAvg * VnAvg));
 
+#if defined(CFD_FAST)
+    double c2 = deltaRho - deltaP * ic2;
+#else
     double c2 = deltaRho - deltaP / (cAvg * cAvg);
+#endif
     Fd[0] += lambda[1] * (c2 * 1.0 + rhoAvg * 0.0);
     // tangential components carry rhoAvg * dv_i, the normal one 0
     // (fluxSchemes.hpp:526-528 for axis normals).
@@ -736,10 +1049,17 @@ CFD_HD void node_flux(const double *p, double *f)
 
 // MidNodeAndNodeDif6 (differ.cpp:54-103): one cell's contribution,
 // (w1 (Fn[i+1]-Fn[i-1]) + w0 (Fh[i+1/2]-Fh[i-1/2]) + w2 (Fh[i+3/2]-Fh[i-3/2])) / h.
-CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fhp1, double fhp3, double h)
+CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fhp1, double fhp3, double h,
+                   double inv_h)
 {
     const double w0 = 3.0 / 2.0, w1 = -3.0 / 10.0, w2 = 1.0 / 30.0;
+#if defined(CFD_FAST)
+    (void)h;
+    return (w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3)) * inv_h;
+#else
+    (void)inv_h;
     return (w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3)) / h;
+#endif
 }
 
 } // namespace cfd

@@ -24,6 +24,7 @@
 // x), so every global access is coalesced along x in all three sweeps.
 #pragma once
 #include "euler_math.cuh"
+#include "mixed.cuh"
 #include "sweep_params.h"
 
 namespace cfd {
@@ -86,7 +87,7 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     }
 }
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W>
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC = 0>
 struct SweepShape {
     static constexpr int NT = S * W;
     static constexpr int R = S + 8;           // prim ring positions
@@ -97,14 +98,18 @@ struct SweepShape {
     static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 };
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W>
-__global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(const SweepParams p)
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+#ifndef CFD_SWEEP_MINB
+#define CFD_SWEEP_MINB 2
+#endif
+__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1) sweep_kernel(const SweepParams p)
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
     constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
     // device-resident loop: the whole launch is a no-op once the loop is done
     if (p.ctl && p.ctl->done) return;
     const double tstage = p.ctl ? p.ctl->tst[p.rk_stage] : p.t;
+    const double inv_h = 1.0 / p.h;
     const double rkBdt = p.ctl ? p.ctl->bdt[p.rk_stage] : p.rkBdt;
     extern __shared__ double smem[];
     double *sp = smem;                   // [NV][W][LSP] prim
@@ -167,18 +172,28 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
 
     // Face j lies between cells j-1 and j (x_{j-1/2}); stencil cells j-3..j+2.
     auto face = [&](int l, int j) {
-        double pr6[6][NV], cs6[6][NV];
+        int slot[6];
 #pragma unroll
-        for (int m = 0; m < 6; m++) {
-            int slot = (j - 3 + m - s_begin + 4) % R;
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                pr6[m][v] = sp[(v * W + l) * LSP + slot];
-                cs6[m][v] = sc[(v * W + l) * LSP + slot];
-            }
-        }
+        for (int m = 0; m < 6; m++) slot[m] = (j - 3 + m - s_begin + 4) % R;
         double fl[NV], fr[NV], fx[NV];
-        reconstruct_face<NV, AX, FAM>(pr6, cs6, p.icst, fl, fr);
+        if constexpr (NV == 3) {
+            double pr6[6][NV], cs6[6][NV];
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    pr6[m][v] = sp[(v * W + l) * LSP + slot[m]];
+                    cs6[m][v] = sc[(v * W + l) * LSP + slot[m]];
+                }
+            }
+            reconstruct_face<NV, AX, FAM>(pr6, cs6, p.icst, fl, fr);
+        } else {
+            const double *spl = sp + l * LSP, *scl = sc + l * LSP;
+            auto csacc = [&](int m, int v) { return scl[v * W * LSP + slot[m]]; };
+            auto pracc = [&](int m, int v) { return spl[v * W * LSP + slot[m]]; };
+            if constexpr (PREC == 1) reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, p.icst, fl, fr);
+            else reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, fl, fr);
+        }
         riemann<NV, AX, FLUX>(fl, fr, fx);
         int fslot = (j - s_begin + 1) % RF;
 #pragma unroll
@@ -228,7 +243,7 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 const double *fv = sf + (v * W + tl) * LSF;
-                double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h);
+                double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
                 double r = p.first ? (0.0 + d) : (p.rhs[gi] + d);
                 if (p.mode != MODE_RK) {
@@ -269,16 +284,21 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? 2 : 1) sweep_kernel(con
     }
 }
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W>
-static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
-    auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC>;
+    // the dynamic shared-memory opt-in is per device
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return e0;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set[dev] = true;
     }
     constexpr int T0 = (AX == 0) ? 1 : 0;
     constexpr int T1 = (AX == 2) ? 1 : 2;
@@ -286,8 +306,19 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
     long long nblk = (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
     if (nblk <= 0) return cudaSuccess;
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    sweep_kernel<NV, AX, FAM, FLUX, S, W><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
+    sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
     return cudaGetLastError();
+}
+
+// FP64 or, in the fast flavour of the multi-dimensional kernels, mixed.
+template <int NV, int AX, int FAM, int FLUX, int S, int W>
+static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
+{
+    if (p.prec == 0) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 0>(p, st);
+#if defined(CFD_FAST)
+    if constexpr (NV >= 4) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 1>(p, st);
+#endif
+    return cudaErrorInvalidValue;
 }
 
 // Tile shapes: along x, 64 cells x 4 lines; along y/z, 8 cells x 32 lines

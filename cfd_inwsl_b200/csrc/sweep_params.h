@@ -69,6 +69,7 @@ struct SweepParams {
     double dm_u, dm_v;  // DoubleMachUp post-shock velocity, 8.25 cos(pi/6) and -8.25 sin(pi/6) from the host libm
     double icst;        // interpolator constant (TENO cutoff)
     int seg_len;        // cells per CTA segment along the sweep
+    int prec;           // 0: FP64 reconstruction, 1: mixed FP32/FP64 (fast flavour only)
 };
 
 // Block-wide max of non-negative doubles followed by one atomicMax per value.

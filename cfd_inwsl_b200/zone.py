@@ -132,6 +132,7 @@ class Info:
         self.dim = self.getDim()
         # GPU-only knobs (no counterpart in the reference)
         self.strict = False     # bitwise-parity build of the kernels
+        self.precision = 0      # 0: FP64, 1: mixed FP32 reconstruction / FP64 state (CFD_PREC_MIXED)
         self.device = 0
         self.seg_len = [0, 0, 0]
 
@@ -202,6 +203,7 @@ class BlockSolver:
         cfg.flux_method = int(info.fluxMethod)
         cfg.diff_method = int(info.diffMethod)
         cfg.strict = int(bool(info.strict))
+        cfg.precision = int(getattr(info, "precision", 0))
         cfg.device = int(info.device)
         types = bc if bc is not None else default_bc_types(info)
         if periodic:

@@ -167,6 +167,11 @@ int cfd_sweep(cfd_handle *h, int idim, int mode, double t);
  * prim -> out[nvar*i ...]) for sweep axis ax. Host pointers; used by tests. */
 int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double *out);
 int cfd_eval_flux(int dim, int ax, int flux_method, int strict, const double *lr, int n, double *out);
+/* Face reconstruction known-answer hook (Recon5Order{1D,2D}EulerEig::reconI,
+ * reconstructor5order.hpp:233-429): n stencils of six cells' prims
+ * (prims6[(6*i + j)*nvar + v]) -> left | right face prims (out[2*nvar*i ...]),
+ * in the reference's operation order (precision 0) or the mixed form (1). */
+int cfd_eval_face(int dim, int ax, int inter_method, int precision, const double *prims6, int n, double *out);
 
 /* Allocation-free RHS evaluation (no counterpart in the reference).
  *

@@ -50,6 +50,7 @@
 #include "eigenSystem.hpp"
 #include "fluxSchemes.hpp"
 #include "interScheme.hpp"
+#include "reconstructor5order.hpp"
 #undef private
 #undef protected
 
@@ -258,6 +259,47 @@ void ref_flux1d(int flux_method, const double *lr6, double *out3)
     std::copy(res.begin(), res.end(), out3);
 }
 
-void ref_set_threads(int n) { omp_set_num_threads(n); }
-
 } // extern "C"
+
+// One face of Recon5Order{1D,2D}EulerEig::reconI (reconstructor5order.hpp:233-429):
+// prims6 = six stencil cells (nvar prims each), face between cells 2 and 3;
+// out = left face prim | right face prim. normal_y selects the 2D normal.
+template <InterpolationScheme5Order F>
+static void recon_one(int dim, int normal_y, const double *prims6, double *out)
+{
+    int nv = dim + 2;
+    std::vector<std::vector<real>> cells(6, std::vector<real>(nv));
+    for (int j = 0; j < 6; j++)
+        for (int v = 0; v < nv; v++) cells[j][v] = prims6[j * nv + v];
+    std::array<std::vector<real>::iterator, 6> in;
+    for (int j = 0; j < 6; j++) in[j] = cells[j].begin();
+    auto run = [&](auto &rc) {
+        rc.nvar = nv;
+        rc.data = std::make_shared<Data>(1, 2 * nv);
+        rc.iter = rc.data->begin();
+        rc.norm = {normal_y ? 0.0 : 1.0, normal_y ? 1.0 : 0.0, 0.0};
+        rc.reconI(in);
+        std::copy(rc.data->begin(), rc.data->end(), out);
+    };
+    if (dim == 1) {
+        Recon5Order1DEulerEig<F> rc;
+        run(rc);
+    } else {
+        Recon5Order2DEulerEig<F> rc;
+        run(rc);
+    }
+}
+
+extern "C" int ref_recon_face(int inter_method, int dim, int normal_y, const double *prims6, double *out)
+{
+    switch (inter_method) {
+    case WCNS5: recon_one<weno5_JSchen>(dim, normal_y, prims6, out); return 0;
+    case WCNSZ5: recon_one<weno5_Z>(dim, normal_y, prims6, out); return 0;
+    case TCNS5: recon_one<Teno5_Z>(dim, normal_y, prims6, out); return 0;
+    case WCNS5CONGZ: recon_one<Teno5_CongZ>(dim, normal_y, prims6, out); return 0;
+    case MUCSLIN5: recon_one<musclIn5>(dim, normal_y, prims6, out); return 0;
+    default: return -1;
+    }
+}
+
+extern "C" void ref_set_threads(int n) { omp_set_num_threads(n); }

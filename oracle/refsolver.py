@@ -58,6 +58,7 @@ def load() -> C.CDLL:
             "ref_flux2d": (None, [C.c_int, vp, C.c_int, vp]),
             "ref_flux1d": (None, [C.c_int, vp, vp]),
             "ref_set_threads": (None, [C.c_int]),
+            "ref_recon_face": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp]),
         }
         for name, (res, args) in protos.items():
             fn = getattr(lib, name)
@@ -186,6 +187,19 @@ def ref_flux(dim: int, ax: int, flux_method: int, lr: np.ndarray) -> np.ndarray:
             lib.ref_flux1d(flux_method, _p(row), _p(o))
         else:
             lib.ref_flux2d(flux_method, _p(row), int(ax == 1), _p(o))
+        out[i] = o
+    return out
+
+
+def ref_recon_face(inter_method: int, dim: int, normal_y: int, prims6: np.ndarray) -> np.ndarray:
+    """The reference's reconI on n six-cell stencils (n x 6 x nvar) -> n x 2 nvar."""
+    lib = load()
+    prims6 = np.ascontiguousarray(prims6, dtype=np.float64)
+    nv = dim + 2
+    out = np.empty((prims6.shape[0], 2 * nv))
+    for i in range(prims6.shape[0]):
+        o = np.empty(2 * nv)
+        assert lib.ref_recon_face(inter_method, dim, normal_y, _p(np.ascontiguousarray(prims6[i])), _p(o)) == 0
         out[i] = o
     return out
 

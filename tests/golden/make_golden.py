@@ -17,6 +17,8 @@ file the reference repository commits:
   rhs_2d.npz                 one RHS, one CFL step and one RK3 step of small 2D
                              grids (random quadrants, smooth periodic field)
   sod_400.npz                1D Sod, 400 cells, WCNS5 + HLLC, CFL 0.5, t = 0.2
+  kat_face.npz               one-face characteristic reconstructions (reconI,
+                             reconstructor5order.hpp:233-429), 1D and 2D, both normals
 """
 from __future__ import annotations
 
@@ -31,7 +33,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
-from oracle.refsolver import RefSolver, ref_flux, ref_inter5  # noqa: E402
+from oracle.refsolver import RefSolver, ref_flux, ref_inter5, ref_recon_face  # noqa: E402
 
 REF_ROOT = Path("/root/reference")
 INTER_METHODS = [2, 3, 8, 9, 10, 11, 12, 13, 15, 22, 23, 35, 37]
@@ -158,6 +160,27 @@ def sod_400():
     return {"cons0": cons0, "cons": r.cons, "dts": dts, "linf": lin}
 
 
+def kat_face(rng):
+    out = {}
+    n = 120
+    for dim in (1, 2):
+        nv = dim + 2
+        P = np.empty((n, 6, nv))
+        P[..., 0] = rng.uniform(0.1, 2.0, (n, 6))
+        P[..., 1:nv - 1] = rng.uniform(-1.5, 1.5, (n, 6, nv - 2))
+        P[..., nv - 1] = rng.uniform(0.05, 2.0, (n, 6))
+        # smooth stencils, shocked stencils and near-vacuum stencils
+        x = np.linspace(0, 1, 6)
+        P[:30] = P[:30, :1] + 0.05 * x[None, :, None] * P[:30, 1:2]
+        P[30:40, 3:, 0] *= 8.0
+        P[40:45, :, nv - 1] *= 1e-6
+        out[f"p{dim}d"] = P
+        for im in (2, 3, 11, 8, 15):
+            for ny in range(dim):
+                out[f"f{dim}d_m{im}_n{ny}"] = ref_recon_face(im, dim, ny, P)
+    return out
+
+
 def main():
     rng = np.random.default_rng(20261203)
     (HERE / "sod_congtcns5ct5_101.json").write_text(json.dumps(sod_log(), indent=0))
@@ -166,6 +189,7 @@ def main():
     np.savez_compressed(HERE / "kat_flux.npz", **kat_flux(rng))
     np.savez_compressed(HERE / "rhs_2d.npz", **rhs_2d(rng))
     np.savez_compressed(HERE / "sod_400.npz", **sod_400())
+    np.savez_compressed(HERE / "kat_face.npz", **kat_face(np.random.default_rng(77)))
     for p in sorted(HERE.glob("*")):
         if p.suffix in (".npz", ".json"):
             print(p.name, p.stat().st_size)

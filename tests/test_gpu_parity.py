@@ -341,3 +341,29 @@ def test_device_loop_output_clipping_vs_reference(ref):
     dts2, _ = s.run_device(max_steps=7)
     np.testing.assert_array_equal(dts2, rd2)
     np.testing.assert_array_equal(s.cons, r.cons)
+
+
+# ----------------------------------------------------------------- face reconstruction KAT
+def test_face_reconstruction_bitwise_against_reference():
+    """reconI of the reference (1D with the positivity limiter, 2D with both
+    normals) against the device reconstruction, strict operation order."""
+    g = np.load(GOLD / "kat_face.npz")
+    for key in g.files:
+        if not key.startswith("f"):
+            continue
+        dim = int(key[1])
+        im = int(key.split("_m")[1].split("_")[0])
+        ax = int(key[-1])
+        out = _lib.eval_face(dim, ax, im, g[f"p{dim}d"])
+        np.testing.assert_array_equal(out, g[key], err_msg=key)
+
+
+def test_mixed_face_close_to_fp64_face():
+    g = np.load(GOLD / "kat_face.npz")
+    P = g["p2d"][:30]  # smooth stencils
+    for im in (2, 11):
+        for ax in (0, 1):
+            f64 = _lib.eval_face(2, ax, im, P)
+            fmx = _lib.eval_face(2, ax, im, P, precision=1)
+            scale = np.abs(P[:, 2:4] - P[:, 2:3]).max() + 1e-30
+            assert np.abs(fmx - f64).max() < 1e-5 * max(scale, 1.0), (im, ax, np.abs(fmx - f64).max())

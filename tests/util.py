@@ -8,7 +8,7 @@ from cfd_inwsl_b200 import zone
 GAMMA = 1.4
 
 
-def make_info(dim, n, zone_=None, im=2, fm=0, strict=False, ncase=0, cfl=0.5, seg_len=(0, 0, 0)):
+def make_info(dim, n, zone_=None, im=2, fm=0, strict=False, ncase=0, cfl=0.5, seg_len=(0, 0, 0), precision=0):
     info = zone.Info()
     info.dim = dim
     n3 = list(n) + [1] * (3 - len(n))
@@ -20,12 +20,13 @@ def make_info(dim, n, zone_=None, im=2, fm=0, strict=False, ncase=0, cfl=0.5, se
     info.nCase = ncase
     info.CFL = cfl
     info.seg_len = list(seg_len)
+    info.precision = precision
     return info
 
 
 def gpu_solver(dim, n, zone_=None, im=2, fm=0, strict=False, ncase=0, periodic=False, bc=None, cfl=0.5,
-               seg_len=(0, 0, 0)):
-    info = make_info(dim, n, zone_, im, fm, strict, ncase, cfl, seg_len)
+               seg_len=(0, 0, 0), precision=0):
+    info = make_info(dim, n, zone_, im, fm, strict, ncase, cfl, seg_len, precision)
     return zone.BlockSolver(info, bc=bc, periodic=periodic)
 
 
