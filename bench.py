@@ -183,6 +183,34 @@ def reference_throughput(dim, n, L, im, fm, cfl, budget_s=12.0, max_steps=50):
                       f"(os.cpu_count() = {os.cpu_count()})"}
 
 
+def vortex_accuracy(n, L, im, fm, cfl, device, t_end=2.0):
+    """L1 density error against the exact translated vortex at t_end, FP64 and
+    mixed, on an n^2 grid of the benchmark configuration."""
+    from cfd_inwsl_b200 import cases, zone
+    out = {"grid": n, "t": t_end}
+    for key, prec in (("fp64", 0), ("mixed", 1)):
+        info = zone.Info()
+        info.dim = 2
+        info.iMax = [n + 1, n + 1, 1]
+        info.calZone = [0, L, 0, L, 0, 0]
+        info.interMethod = im
+        info.fluxMethod = fm
+        info.CFL = cfl
+        info.precision = prec
+        info.device = device
+        info.endStep = 1
+        info.outputDt = t_end
+        s = zone.BlockSolver(info, periodic=True)
+        c, _ = cases.isentropic_vortex(n, L=L)
+        s.set_cons(c)
+        s.run_device()
+        exact, _ = cases.isentropic_vortex(n, t=t_end, L=L)
+        out[key] = float(np.abs(s.cons[:, 0] - exact[:, 0]).mean())
+        s.close()
+    out["ratio_mixed_over_fp64"] = out["mixed"] / out["fp64"]
+    return out
+
+
 # --------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -306,6 +334,32 @@ def run_ours(args, rank, world, local_rank):
     e2e_value = world * ncell * e2e_steps / (e2e_ms / 1e3)
     state_bytes = ncell * (dim + 2) * 8
 
+    # ---- the mixed FP32/FP64 form on the same workload, and both forms' accuracy
+    mixed = None
+    if not args.no_mixed:
+        info_m = zone.Info()
+        for k, v in vars(info).items():
+            setattr(info_m, k, v)
+        info_m.precision = 1
+        sm = zone.BlockSolver(info_m, periodic=True)
+        _lib.check(lib.cfd_set_stream(sm.h, C.c_void_p(stream.cuda_stream)), sm.h)
+        sm.set_cons(c)
+        tm = C.c_double(0.0)
+        nm = C.c_int(0)
+        _lib.check(lib.cfd_run(sm.h, cfl, 1, 1e300, args.warmup, C.byref(tm), C.byref(nm), None, None), sm.h)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _lib.check(lib.cfd_run(sm.h, cfl, 1, 1e300, args.steps, C.byref(tm), C.byref(nm), None, None), sm.h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_m = max_over_ranks(e0.elapsed_time(e1))
+        sm.close()
+        value_m = world * ncell * args.steps / (ms_m / 1e3)
+        mixed = {"value": value_m, "unit": "cell-steps/s", "ms_per_step": ms_m / args.steps,
+                 "speedup_vs_fp64": value_m / value}
+        if dim == 2 and rank == 0:
+            mixed["l1_rho_vs_exact"] = vortex_accuracy(args.accuracy_grid, L, im, fm, cfl, local_rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_throughput(dim, n, L, im, fm, cfl, budget_s=args.cpu_budget)
@@ -331,6 +385,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if mixed is not None:
+        result["mixed"] = mixed
     if cpu is not None:
         result["cpu_baseline"] = cpu
     solver.close()
@@ -346,6 +402,8 @@ def main():
     ap.add_argument("--workload", default="vortex2048", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--accuracy-grid", type=int, default=512)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

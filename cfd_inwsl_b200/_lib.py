@@ -75,6 +75,7 @@ _PROTOS = {
     "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_version": (C.c_char_p, []),
+    "cfd_accuracy_test": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "cfd_eval_face": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_launch_count": (C.c_ulonglong, [C.c_void_p]),
@@ -144,4 +145,13 @@ def eval_face(dim: int, ax: int, inter_method: int, prims6: np.ndarray, precisio
     n = prims6.shape[0]
     out = np.empty((n, 2 * (dim + 2)))
     check(load().cfd_eval_face(dim, ax, inter_method, precision, ptr(prims6), n, ptr(out)))
+    return out
+
+
+def accuracy_derivative(inter_method: int, q_with_ghosts: np.ndarray, h: float) -> np.ndarray:
+    """Device d q / d x of the AccuracyTest composition (see cfd_accuracy_test)."""
+    q = np.ascontiguousarray(q_with_ghosts, dtype=np.float64)
+    n = q.size - 8
+    out = np.empty(n)
+    check(load().cfd_accuracy_test(inter_method, n, float(h), ptr(q), ptr(out)))
     return out

@@ -140,6 +140,20 @@ __global__ void eval_flux_kernel(const double *lr, int n, double *out)
     }
 }
 
+// Scalar accuracy test: face values by the left-biased five-point interpolation
+// of q (the upwind face flux of a unit-speed scalar), node fluxes = q, MND6
+// difference: d q / d x at the n cells. q holds 4 ghost values on each side.
+template <int FAM>
+__global__ void accuracy_kernel(const double *q, int n, double h, double c, double *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double *g = q + 4;  // g[k] = value at cell k, k in [-4, n+3]
+    // face x_{k+1/2} from cells k-2 .. k+2
+    auto face = [&](int k) { return cfd::inter5<FAM>(g[k - 2], g[k - 1], g[k], g[k + 1], g[k + 2], c); };
+    out[i] = cfd::mnd6(g[i - 1], g[i + 1], face(i - 2), face(i - 1), face(i), face(i + 1), h, 1.0 / h);
+}
+
 // One face reconstruction per thread from six stencil prims (known-answer hook).
 template <int NV, int AX, int FAM, int PREC>
 __global__ void eval_face_kernel(const double *prims6, int n, double c, double *out)
@@ -998,6 +1012,32 @@ extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, c
 #undef CFD_EFACE
     cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * 2 * nv * n, cudaMemcpyDeviceToHost);
     cudaFree(din);
+    cudaFree(dout);
+    return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
+}
+
+extern "C" int cfd_accuracy_test(int inter_method, int n, double h, const double *q, double *dqdx)
+{
+    InterMap im = map_inter_method(inter_method, 1);
+    if (!im.ok) return CFD_ERR_UNSUPPORTED;
+    if (n < 1 || !(h > 0)) return CFD_ERR_CONFIG;
+    double *dq = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dq, sizeof(double) * (n + 8)) != cudaSuccess) return CFD_ERR_NOMEM;
+    if (cudaMalloc(&dout, sizeof(double) * n) != cudaSuccess) {
+        cudaFree(dq);
+        return CFD_ERR_NOMEM;
+    }
+    cudaMemcpy(dq, q, sizeof(double) * (n + 8), cudaMemcpyHostToDevice);
+    int g = (n + 127) / 128;
+    switch (im.fam) {
+    case cfd::FAM_WCNS5: accuracy_kernel<cfd::FAM_WCNS5><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    case cfd::FAM_WENOZ: accuracy_kernel<cfd::FAM_WENOZ><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    case cfd::FAM_TENOZ: accuracy_kernel<cfd::FAM_TENOZ><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    case cfd::FAM_TENOCONG: accuracy_kernel<cfd::FAM_TENOCONG><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    default: accuracy_kernel<cfd::FAM_MUSCL><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    }
+    cudaError_t e = cudaMemcpy(dqdx, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dq);
     cudaFree(dout);
     return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
 }

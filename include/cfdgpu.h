@@ -198,6 +198,12 @@ int cfd_eval_face(int dim, int ax, int inter_method, int precision, const double
 #define CFD_NOALLOC_MAX_LINE_ENDS 16384
 int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, double *rhs_soa, double t, void *stream);
 
+/* Order-of-accuracy hook (the reference's AccuracyTest, CongFD1.0/AccuracyTest.cpp:14-83):
+ * d q / d x at n cells of spacing h for a unit-speed scalar, face values by the
+ * left-biased five-point interpolation of inter_method, node values = q, MND6
+ * difference. q holds n + 8 values: 4 ghosts, the n cells, 4 ghosts. */
+int cfd_accuracy_test(int inter_method, int n, double h, const double *q, double *dqdx);
+
 /* Library version string. */
 const char *cfd_version(void);
 
