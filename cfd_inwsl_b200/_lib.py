@@ -75,6 +75,13 @@ _PROTOS = {
     "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_version": (C.c_char_p, []),
+    "cfd_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cfd_batch_destroy": (None, [C.c_void_p]),
+    "cfd_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "cfd_batch_case": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cfd_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_batch_launch_count": (C.c_ulonglong, [C.c_void_p]),
+    "cfd_batch_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "cfd_accuracy_test": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "cfd_eval_face": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

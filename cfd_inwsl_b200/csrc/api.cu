@@ -1053,3 +1053,336 @@ bool map_inter_method_for(int inter_method, int dim, int *fam, double *c)
     return true;
 }
 } // namespace cfd
+
+// ===================================================================== batch
+// Many independent cases advanced together: one persistent sweep launch per
+// direction and stage covers the tiles of every unfinished case, and one
+// control kernel advances every case's own stepsLoopCFL state (own dt,
+// own output clipping, own step count).
+
+namespace {
+
+__global__ void batch_step_begin_kernel(cfd::StepCtl *ctl, unsigned long long *const *reds, int ncases, int dim,
+                                        int *active)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncases) return;
+    cfd::StepCtl *cc = ctl + c;
+    if (cc->done) return;
+    if (!(cc->step < cc->endStep && cc->k < cc->maxSteps)) {
+        cc->done = 1;
+        return;
+    }
+    unsigned long long *red = reds[c];
+    double lambda = 0;
+    for (int d = 0; d < dim; d++) lambda += __longlong_as_double((long long)red[1 + d]);
+    double dt = cc->cfl / lambda;
+    if (cc->outputT + dt > cc->outputDt) {
+        dt = cc->outputDt - cc->outputT;
+        cc->outputT = 0.0;
+        cc->step++;
+    } else
+        cc->outputT += dt;
+    cc->dt = dt;
+    cc->bdt[1] = dt;
+    cc->bdt[2] = 0.25 * dt;
+    cc->bdt[3] = 2.0 / 3.0 * dt;
+    cc->tst[1] = cc->t;
+    cc->tst[2] = cc->t + dt;
+    cc->tst[3] = cc->tst[2] - dt / 2;
+    for (int i = 0; i < 4; i++) red[i] = 0ULL;
+    atomicAdd(active, 1);
+}
+
+__global__ void batch_step_end_kernel(cfd::StepCtl *ctl, int ncases)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncases) return;
+    cfd::StepCtl *cc = ctl + c;
+    if (cc->done) return;
+    double dt = cc->dt;
+    cc->t = (((cc->t + dt) - dt / 2) - dt / 2) + dt;
+    cc->k++;
+}
+
+} // namespace
+
+struct cfd_batch {
+    std::vector<cfd_handle *> h;
+    int ncases = 0, dim = 0, nv = 0, fam = 0, flux = 0, prec = 0;
+    bool strict = false;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    cfd::StepCtl *ctl = nullptr, *ctl_host = nullptr;
+    unsigned long long **d_reds = nullptr;
+    int *d_active = nullptr;
+    // params[(slot * 3 + (stage - 1)) * dim + d][case]
+    std::vector<SweepParams> params_host;
+    SweepParams *d_params = nullptr;
+    long long *d_tile_start = nullptr;  // [dim][ncases + 1]
+    std::vector<long long> tile_total;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    unsigned long long launches = 0;
+    std::string msg;
+};
+
+namespace {
+
+int bfail(cfd_batch *b, int code, const std::string &m)
+{
+    if (b) b->msg = m;
+    return code;
+}
+
+#define CFD_BCUDA(b, call)                                                         \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) return bfail(b, CFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Parameter block of case c for the sweep along d in stage `stage`, with the
+// state buffers taken `slot` steps after the case's current slot.
+SweepParams batch_params(cfd_batch *b, int c, int slot, int stage, int d)
+{
+    cfd_handle *h = b->h[c];
+    int cur = (h->cur + slot) % 3;
+    double *U0 = h->u[cur], *U1 = h->u[(cur + 1) % 3], *U2 = h->u[(cur + 2) % 3];
+    SweepParams p = base_params(h, d);
+    const double *uin = stage == 1 ? U0 : stage == 2 ? U1 : U2;
+    double *uout = stage == 2 ? U2 : U1;
+    bool last = (d == b->dim - 1);
+    p.u = uin;
+    p.u0 = U0;
+    p.rhs = h->rhs;
+    p.u_out = uout;
+    p.mode = last ? cfd::MODE_RK : cfd::MODE_WRITE;
+    p.first = (d == 0);
+    p.rk_stage = stage;
+    p.rkA = stage == 1 ? 1.0 : stage == 2 ? 0.75 : 1.0 / 3.0;
+    p.rkC = stage == 1 ? 0.0 : stage == 2 ? 0.25 : 2.0 / 3.0;
+    p.want_reduce = (stage == 3 && last) ? 1 : 0;
+    p.ctl = b->ctl + c;
+    return p;
+}
+
+int batch_enqueue_step(cfd_batch *b, int slot)
+{
+    int g = (b->ncases + 127) / 128;
+    batch_step_begin_kernel<<<g, 128, 0, b->stream>>>(b->ctl, b->d_reds, b->ncases, b->dim, b->d_active);
+    CFD_BCUDA(b, cudaGetLastError());
+    for (int stage = 1; stage <= 3; stage++) {
+        for (int d = 0; d < b->dim; d++) {
+            cfd::BatchSweep bs;
+            bs.cases = b->d_params + (size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases;
+            bs.tile_start = b->d_tile_start + (size_t)d * (b->ncases + 1);
+            bs.ncases = b->ncases;
+            bs.total_tiles = b->tile_total[d];
+            bs.num_sms = b->num_sms;
+            bs.prec = b->prec;
+            cudaError_t e = cfd::launch_sweep_batched_any(b->strict, b->nv, b->fam, d, b->flux, bs, b->stream);
+            if (e != cudaSuccess) return bfail(b, CFD_ERR_CUDA, std::string("batched sweep: ") + cudaGetErrorString(e));
+        }
+    }
+    batch_step_end_kernel<<<g, 128, 0, b->stream>>>(b->ctl, b->ncases);
+    CFD_BCUDA(b, cudaGetLastError());
+    return CFD_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int cfd_batch_create(const cfd_config *cfgs, int ncases, cfd_batch **out)
+{
+    if (!cfgs || !out || ncases < 1) return CFD_ERR_CONFIG;
+    *out = nullptr;
+    for (int c = 1; c < ncases; c++) {
+        const cfd_config &a = cfgs[0], &z = cfgs[c];
+        if (a.dim != z.dim || a.inter_method != z.inter_method || a.flux_method != z.flux_method ||
+            a.strict != z.strict || a.precision != z.precision || a.device != z.device)
+            return CFD_ERR_CONFIG;  // one kernel instantiation serves the batch
+    }
+    cfd_batch *b = new cfd_batch();
+    b->ncases = ncases;
+    for (int c = 0; c < ncases; c++) {
+        cfd_config cc = cfgs[c];
+        for (int d = 0; d < 3; d++)
+            if (cc.seg_len[d] <= 0) cc.seg_len[d] = cc.n[d];  // whole lines: the batch has tiles to spare
+        cfd_handle *h = nullptr;
+        int rc = cfd_create(&cc, &h);
+        if (rc) {
+            cfd_batch_destroy(b);
+            return rc;
+        }
+        b->h.push_back(h);
+    }
+    cfd_handle *h0 = b->h[0];
+    b->dim = h0->dim;
+    b->nv = h0->nv;
+    b->fam = h0->fam;
+    b->flux = h0->cfg.flux_method;
+    b->strict = h0->strict;
+    b->prec = h0->cfg.precision == CFD_PREC_MIXED ? 1 : 0;
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, h0->cfg.device);
+    auto bail = [&](cudaError_t e) {
+        fprintf(stderr, "cfd_batch_create: %s\n", cudaGetErrorString(e));
+        cfd_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? CFD_ERR_NOMEM : CFD_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    b->stream = b->own_stream;
+    if ((e = cudaMalloc(&b->ctl, sizeof(cfd::StepCtl) * ncases)) != cudaSuccess) return bail(e);
+    if ((e = cudaMallocHost(&b->ctl_host, sizeof(cfd::StepCtl) * ncases)) != cudaSuccess) return bail(e);
+    if ((e = cudaMalloc(&b->d_reds, sizeof(unsigned long long *) * ncases)) != cudaSuccess) return bail(e);
+    if ((e = cudaMalloc(&b->d_active, sizeof(int))) != cudaSuccess) return bail(e);
+    std::vector<unsigned long long *> reds(ncases);
+    for (int c = 0; c < ncases; c++) reds[c] = b->h[c]->red;
+    if ((e = cudaMemcpy(b->d_reds, reds.data(), sizeof(void *) * ncases, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e);
+    size_t np = (size_t)9 * b->dim * ncases;
+    b->params_host.resize(np);
+    if ((e = cudaMalloc(&b->d_params, sizeof(SweepParams) * np)) != cudaSuccess) return bail(e);
+    std::vector<long long> ts((size_t)b->dim * (ncases + 1));
+    b->tile_total.assign(b->dim, 0);
+    for (int d = 0; d < b->dim; d++) {
+        long long acc = 0;
+        for (int c = 0; c < ncases; c++) {
+            ts[(size_t)d * (ncases + 1) + c] = acc;
+            acc += cfd::sweep_tile_count(b->nv, d, base_params(b->h[c], d));
+        }
+        ts[(size_t)d * (ncases + 1) + ncases] = acc;
+        b->tile_total[d] = acc;
+    }
+    if ((e = cudaMalloc(&b->d_tile_start, sizeof(long long) * ts.size())) != cudaSuccess) return bail(e);
+    if ((e = cudaMemcpy(b->d_tile_start, ts.data(), sizeof(long long) * ts.size(), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return bail(e);
+    *out = b;
+    return CFD_OK;
+}
+
+void cfd_batch_destroy(cfd_batch *b)
+{
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (cfd_handle *h : b->h) cfd_destroy(h);
+    cudaFree(b->ctl);
+    if (b->ctl_host) cudaFreeHost(b->ctl_host);
+    cudaFree(b->d_reds);
+    cudaFree(b->d_active);
+    cudaFree(b->d_params);
+    cudaFree(b->d_tile_start);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    delete b;
+}
+
+const char *cfd_batch_last_error(const cfd_batch *b) { return b ? b->msg.c_str() : "null batch"; }
+
+int cfd_batch_case(cfd_batch *b, int c, cfd_handle **h)
+{
+    if (!b || !h || c < 0 || c >= b->ncases) return CFD_ERR_CONFIG;
+    *h = b->h[c];
+    return CFD_OK;
+}
+
+int cfd_batch_set_stream(cfd_batch *b, void *stream)
+{
+    if (!b) return CFD_ERR_CONFIG;
+    CFD_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+    return CFD_OK;
+}
+
+unsigned long long cfd_batch_launch_count(const cfd_batch *b) { return b ? b->launches : 0; }
+
+int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_dt, int max_steps, double *t,
+                  int *nsteps)
+{
+    if (!b || !output_dt || !t || !nsteps || max_steps < 0 || end_step < 0) return CFD_ERR_CONFIG;
+    for (int c = 0; c < b->ncases; c++) nsteps[c] = 0;
+    if (max_steps == 0 || end_step == 0) return CFD_OK;
+    // every case's boundary tables and initial wave speeds on the handle streams
+    for (int c = 0; c < b->ncases; c++) {
+        cfd_handle *h = b->h[c];
+        int rc = sync_bc(h);
+        if (rc) return bfail(b, rc, h->msg);
+        if (!h->ws_valid && (rc = launch_wave_speed(h))) return bfail(b, rc, h->msg);
+        CFD_BCUDA(b, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+        CFD_BCUDA(b, cudaStreamSynchronize(h->stream));
+    }
+    // parameter blocks for the three buffer rotations, stages and directions
+    for (int slot = 0; slot < 3; slot++)
+        for (int stage = 1; stage <= 3; stage++)
+            for (int d = 0; d < b->dim; d++)
+                for (int c = 0; c < b->ncases; c++)
+                    b->params_host[(size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases + c] =
+                        batch_params(b, c, slot, stage, d);
+    CFD_BCUDA(b, cudaMemcpyAsync(b->d_params, b->params_host.data(), sizeof(SweepParams) * b->params_host.size(),
+                                 cudaMemcpyHostToDevice, b->stream));
+    for (int c = 0; c < b->ncases; c++) {
+        cfd::StepCtl &cc = b->ctl_host[c];
+        std::memset(&cc, 0, sizeof(cc));
+        cc.t = t[c];
+        cc.outputDt = output_dt[c];
+        cc.cfl = cfl;
+        cc.endStep = end_step;
+        cc.maxSteps = max_steps;
+    }
+    CFD_BCUDA(b, cudaMemcpyAsync(b->ctl, b->ctl_host, sizeof(cfd::StepCtl) * b->ncases, cudaMemcpyHostToDevice,
+                                 b->stream));
+    // graph of 3 steps (the buffers return to their roles after each graph)
+    const int G = 3;
+    if (!b->graph) {
+        cudaGraph_t g;
+        CFD_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = CFD_OK;
+        for (int s = 0; s < G && rc == CFD_OK; s++) rc = batch_enqueue_step(b, s);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return bfail(b, CFD_ERR_CUDA, cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return bfail(b, CFD_ERR_CUDA, cudaGetErrorString(e));
+        b->graph_steps = G;
+    }
+    int launched = 0, quota = 3;
+    int active = 0;
+    const unsigned long long per_step = 2 + 3ULL * b->dim;
+    while (launched < max_steps) {
+        CFD_BCUDA(b, cudaMemsetAsync(b->d_active, 0, sizeof(int), b->stream));
+        for (int q = 0; q < quota && launched < max_steps; q += G) {
+            CFD_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+            b->launches += per_step * G;
+            launched += G;
+        }
+        CFD_BCUDA(b, cudaMemcpyAsync(&active, b->d_active, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        CFD_BCUDA(b, cudaStreamSynchronize(b->stream));
+        if (active == 0) break;  // no case took a step in the last batch of graphs
+        if (quota < (1 << 16)) quota *= 2;
+    }
+    CFD_BCUDA(b, cudaMemcpyAsync(b->ctl_host, b->ctl, sizeof(cfd::StepCtl) * b->ncases, cudaMemcpyDeviceToHost,
+                                 b->stream));
+    CFD_BCUDA(b, cudaStreamSynchronize(b->stream));
+    int rc = CFD_OK;
+    for (int c = 0; c < b->ncases; c++) {
+        cfd_handle *h = b->h[c];
+        int k = b->ctl_host[c].k;
+        nsteps[c] = k;
+        t[c] = b->ctl_host[c].t;
+        h->cur = (h->cur + k) % 3;
+        h->ws_valid = true;
+        unsigned err = 0;
+        CFD_BCUDA(b, cudaMemcpy(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost));
+        int r = check_err(h, err);
+        if (r && !rc) {
+            rc = r;
+            b->msg = "case " + std::to_string(c) + ": " + h->msg;
+        }
+    }
+    return rc;
+}
+
+} // extern "C"

@@ -102,7 +102,7 @@ template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
 #ifndef CFD_SWEEP_MINB
 #define CFD_SWEEP_MINB 2
 #endif
-__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1) sweep_kernel(const SweepParams p)
+__device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
     constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1) swe
     const int nt0 = p.n[T0];
     const int nseg = (nd + p.seg_len - 1) / p.seg_len;
     const int nblk0 = (nt0 + W - 1) / W;
-    int bid = blockIdx.x;
+    int bid = block_id;
     const int seg = bid % nseg;
     bid /= nseg;
     const int a0 = (bid % nblk0) * W;
@@ -285,6 +285,58 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1) swe
 }
 
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
+    sweep_kernel(const __grid_constant__ SweepParams p)
+{
+    sweep_tile<NV, AX, FAM, FLUX, S, W, PREC>(p, blockIdx.x);
+}
+
+// Number of CTA tiles one case's sweep along AX needs.
+template <int AX, int W>
+__host__ __device__ inline long long sweep_tiles(const SweepParams &p)
+{
+    constexpr int T0 = (AX == 0) ? 1 : 0;
+    constexpr int T1 = (AX == 2) ? 1 : 2;
+    long long nseg = (p.n[AX] + p.seg_len - 1) / p.seg_len;
+    return (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
+}
+
+// Persistent sweep over many independent cases: the tiles of all cases form
+// one work list (tile_start[c] = first tile of case c, prefix sums); each CTA
+// walks the list with a grid stride, copies its case's parameter block to
+// shared memory and runs the same tile code as sweep_kernel. Cases whose
+// device loop is done are skipped tile by tile.
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
+    sweep_batched_kernel(const SweepParams *__restrict__ cases, const long long *__restrict__ tile_start, int ncases)
+{
+    __shared__ SweepParams sp;
+    __shared__ int s_case;
+    const long long total = tile_start[ncases];
+    for (long long item = blockIdx.x; item < total; item += gridDim.x) {
+        __syncthreads();  // the previous tile is done with sp
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = ncases - 1;  // last case with tile_start <= item
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (tile_start[mid] <= item) lo = mid; else hi = mid - 1;
+            }
+            s_case = lo;
+        }
+        __syncthreads();
+        const int c = s_case;
+        {
+            const int words = (int)(sizeof(SweepParams) / sizeof(int));
+            const int *src = reinterpret_cast<const int *>(cases + c);
+            int *dst = reinterpret_cast<int *>(&sp);
+            for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+        }
+        __syncthreads();
+        sweep_tile<NV, AX, FAM, FLUX, S, W, PREC>(sp, (int)(item - tile_start[c]));
+    }
+}
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
 static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
@@ -308,6 +360,43 @@ static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
     return cudaGetLastError();
+}
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+static cudaError_t launch_batched_shape_p(const BatchSweep &b, cudaStream_t st)
+{
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    auto kern = sweep_batched_kernel<NV, AX, FAM, FLUX, S, W, PREC>;
+    static bool attr_set[64] = {};
+    static int blocks_per_sm[64] = {};
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return e0;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm[dev], kern, SH::NT, SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        if (blocks_per_sm[dev] < 1) blocks_per_sm[dev] = 1;
+        attr_set[dev] = true;
+    }
+    long long grid = (long long)b.num_sms * blocks_per_sm[dev];
+    if (b.total_tiles < grid) grid = b.total_tiles;
+    if (grid <= 0) return cudaSuccess;
+    sweep_batched_kernel<NV, AX, FAM, FLUX, S, W, PREC>
+        <<<(unsigned)grid, SH::NT, SH::SMEM_BYTES, st>>>(b.cases, b.tile_start, b.ncases);
+    return cudaGetLastError();
+}
+
+template <int NV, int AX, int FAM, int FLUX, int S, int W>
+static cudaError_t launch_batched_shape(const BatchSweep &b, cudaStream_t st)
+{
+    if (b.prec == 0) return launch_batched_shape_p<NV, AX, FAM, FLUX, S, W, 0>(b, st);
+#if defined(CFD_FAST)
+    if constexpr (NV >= 4) return launch_batched_shape_p<NV, AX, FAM, FLUX, S, W, 1>(b, st);
+#endif
+    return cudaErrorInvalidValue;
 }
 
 // FP64 or, in the fast flavour of the multi-dimensional kernels, mixed.
@@ -341,6 +430,30 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
             if (ax == 2)
                 return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, 8, 32>(p, st)
                                          : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, 8, 32>(p, st);
+        }
+        return cudaErrorInvalidValue;
+    }
+}
+
+// Persistent batched sweep (2D and 3D; same tile shapes as launch_sweep).
+template <int NV, int FAM>
+cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStream_t st)
+{
+    if constexpr (NV == 3) {
+        if (ax != 0) return cudaErrorInvalidValue;
+        return flux == FLUX_HLLC ? launch_batched_shape<3, 0, FAM, FLUX_HLLC, 128, 1>(b, st)
+                                 : launch_batched_shape<3, 0, FAM, FLUX_ROE, 128, 1>(b, st);
+    } else {
+        if (ax == 0)
+            return flux == FLUX_HLLC ? launch_batched_shape<NV, 0, FAM, FLUX_HLLC, 64, 4>(b, st)
+                                     : launch_batched_shape<NV, 0, FAM, FLUX_ROE, 64, 4>(b, st);
+        if (ax == 1)
+            return flux == FLUX_HLLC ? launch_batched_shape<NV, 1, FAM, FLUX_HLLC, 8, 32>(b, st)
+                                     : launch_batched_shape<NV, 1, FAM, FLUX_ROE, 8, 32>(b, st);
+        if constexpr (NV == 5) {
+            if (ax == 2)
+                return flux == FLUX_HLLC ? launch_batched_shape<NV, 2, FAM, FLUX_HLLC, 8, 32>(b, st)
+                                         : launch_batched_shape<NV, 2, FAM, FLUX_ROE, 8, 32>(b, st);
         }
         return cudaErrorInvalidValue;
     }

@@ -72,6 +72,17 @@ struct SweepParams {
     int prec;           // 0: FP64 reconstruction, 1: mixed FP32/FP64 (fast flavour only)
 };
 
+// One batched sweep launch: the parameter blocks of every case (device array)
+// and the prefix sums of their tile counts (ncases + 1 entries, device array).
+struct BatchSweep {
+    const SweepParams *cases;
+    const long long *tile_start;
+    int ncases;
+    long long total_tiles;
+    int num_sms;
+    int prec;
+};
+
 // Block-wide max of non-negative doubles followed by one atomicMax per value.
 // NaN inputs are ignored (fmax), like the reference's comparisons that never
 // let a NaN replace the running maximum.

@@ -176,6 +176,34 @@ def default_bc_types(info: Info) -> list[list[int]]:
     return bc
 
 
+def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
+    """cfd_config from an Info, with the Initializer::initBnds boundary types
+    unless bc ([[lo, hi], ...]) or periodic=True overrides them."""
+    lib = _lib.load()
+    n = info.icMax()
+    cfg = _lib.CfdConfig()
+    lib.cfd_config_default(C.byref(cfg))
+    cfg.dim = info.dim
+    for d in range(3):
+        cfg.n[d] = n[d] if d < info.dim else 1
+        cfg.h[d] = info.geth(d)
+        cfg.x0[d] = info.calZone[2 * d]
+        cfg.seg_len[d] = int(info.seg_len[d])
+    cfg.inter_method = int(info.interMethod)
+    cfg.flux_method = int(info.fluxMethod)
+    cfg.diff_method = int(info.diffMethod)
+    cfg.strict = int(bool(info.strict))
+    cfg.precision = int(getattr(info, "precision", 0))
+    cfg.device = int(info.device)
+    types = bc if bc is not None else default_bc_types(info)
+    if periodic:
+        types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]
+    for d in range(3):
+        for s in range(2):
+            cfg.bc[d][s] = int(types[d][s])
+    return cfg
+
+
 class BlockSolver:
     """GPU counterpart of BlockSolver (blockSolver.hpp:7-57) for the Euler path.
 
@@ -191,26 +219,7 @@ class BlockSolver:
         self.n = info.icMax()
         self.ncell = self.n[0] * self.n[1] * self.n[2]
         self.timesteps = 0
-        cfg = _lib.CfdConfig()
-        self.lib.cfd_config_default(C.byref(cfg))
-        cfg.dim = info.dim
-        for d in range(3):
-            cfg.n[d] = self.n[d] if d < info.dim else 1
-            cfg.h[d] = info.geth(d)
-            cfg.x0[d] = info.calZone[2 * d]
-            cfg.seg_len[d] = int(info.seg_len[d])
-        cfg.inter_method = int(info.interMethod)
-        cfg.flux_method = int(info.fluxMethod)
-        cfg.diff_method = int(info.diffMethod)
-        cfg.strict = int(bool(info.strict))
-        cfg.precision = int(getattr(info, "precision", 0))
-        cfg.device = int(info.device)
-        types = bc if bc is not None else default_bc_types(info)
-        if periodic:
-            types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]
-        for d in range(3):
-            for s in range(2):
-                cfg.bc[d][s] = int(types[d][s])
+        cfg = make_config(info, bc, periodic)
         self.cfg = cfg
         h = C.c_void_p()
         rc = self.lib.cfd_create(C.byref(cfg), C.byref(h))
@@ -329,6 +338,74 @@ class BlockSolver:
         info.t = t.value
         self.timesteps += ns.value
         return dts[: ns.value], lin[: ns.value]
+
+
+class BlockBatch:
+    """Many independent BlockSolver cases advanced together (cfd_batch_*).
+
+    infos: one Info per case (same dim, scheme, flux, flavour, precision);
+    grids, spacings and boundaries may differ."""
+
+    def __init__(self, infos, bc=None, periodic: bool = False):
+        self.lib = _lib.load()
+        self.infos = list(infos)
+        n = len(self.infos)
+        cfgs = (_lib.CfdConfig * n)()
+        for i, info in enumerate(self.infos):
+            cfgs[i] = make_config(info, bc, periodic)
+        h = C.c_void_p()
+        rc = self.lib.cfd_batch_create(cfgs, n, C.byref(h))
+        if rc != 0:
+            raise _lib.CfdError(rc, "cfd_batch_create")
+        self.h = h
+        self.ncases = n
+        self.cases = []
+        for i in range(n):
+            ch = C.c_void_p()
+            _lib.check(self.lib.cfd_batch_case(self.h, i, C.byref(ch)))
+            self.cases.append(ch)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cfd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _shape(self, i):
+        info = self.infos[i]
+        n = info.icMax()
+        return n[0] * n[1] * n[2], info.nPrim()
+
+    def set_cons(self, i, cons):
+        nc, nv = self._shape(i)
+        a = np.ascontiguousarray(cons, dtype=np.float64).reshape(nc, nv)
+        _lib.check(self.lib.cfd_upload_cons(self.cases[i], _lib.ptr(a)), self.cases[i])
+
+    def cons(self, i) -> np.ndarray:
+        nc, nv = self._shape(i)
+        out = np.empty((nc, nv))
+        _lib.check(self.lib.cfd_download_cons(self.cases[i], _lib.ptr(out)), self.cases[i])
+        return out
+
+    def run(self, output_dt, end_step: int = 1, max_steps: int = 1 << 30, cfl: float = None):
+        """Advance every case (stepsLoopCFL per case); returns (t, nsteps) arrays."""
+        od = np.ascontiguousarray(np.broadcast_to(np.asarray(output_dt, dtype=np.float64), (self.ncases,)))
+        t = np.ascontiguousarray([info.t for info in self.infos], dtype=np.float64)
+        ns = np.zeros(self.ncases, dtype=np.int32)
+        cfl = self.infos[0].CFL if cfl is None else cfl
+        rc = self.lib.cfd_batch_run(self.h, float(cfl), int(end_step), _lib.ptr(od), int(max_steps), _lib.ptr(t),
+                                    _lib.ptr(ns))
+        if rc != 0:
+            m = self.lib.cfd_batch_last_error(self.h)
+            raise _lib.CfdError(rc, m.decode() if m else "")
+        for info, tt in zip(self.infos, t):
+            info.t = float(tt)
+        return t, ns
 
 
 def sod_1d(info: Info) -> np.ndarray:

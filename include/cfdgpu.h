@@ -204,6 +204,28 @@ int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, double *rhs_s
  * difference. q holds n + 8 values: 4 ghosts, the n cells, 4 ghosts. */
 int cfd_accuracy_test(int inter_method, int n, double h, const double *q, double *dqdx);
 
+/* Batched mode: many independent cases of uneven grid sizes advanced
+ * together. The configurations must share dim, inter_method, flux_method,
+ * strict, precision and device; grid sizes, spacing and boundaries may differ.
+ * Each step is one persistent sweep launch per direction and stage over the
+ * tiles of every unfinished case and one control kernel for all cases; steps
+ * are captured in CUDA graphs. Each case keeps its own dt, output clipping and
+ * step count (BlockSolver::stepsLoopCFL per case). */
+typedef struct cfd_batch cfd_batch;
+int cfd_batch_create(const cfd_config *cfgs, int ncases, cfd_batch **out);
+void cfd_batch_destroy(cfd_batch *b);
+const char *cfd_batch_last_error(const cfd_batch *b);
+/* The handle of case c, for cfd_upload_cons / cfd_download_cons /
+ * cfd_set_line_bc on that case (owned by the batch). */
+int cfd_batch_case(cfd_batch *b, int c, cfd_handle **h);
+int cfd_batch_set_stream(cfd_batch *b, void *stream);
+unsigned long long cfd_batch_launch_count(const cfd_batch *b);
+/* Runs every case until it finished end_step output intervals of
+ * output_dt[c] or max_steps steps; t[c] is each case's start time on entry
+ * and end time on return; nsteps[c] its step count. */
+int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_dt, int max_steps, double *t,
+                  int *nsteps);
+
 /* Library version string. */
 const char *cfd_version(void);
 
