@@ -48,6 +48,7 @@ class CfdConfig(C.Structure):
         ("bc", (C.c_int * 2) * 3),
         ("device", C.c_int),
         ("seg_len", C.c_int * 3),
+        ("source_type", C.c_int),
     ]
 
 

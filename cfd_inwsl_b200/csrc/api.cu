@@ -441,6 +441,7 @@ int rhs_all(cfd_handle *h, const double *u, double t)
         p.mode = cfd::MODE_WRITE;
         p.first = (d == 0);
         p.t = t;
+        p.gravity = (h->cfg.source_type == 1 && d == h->dim - 1) ? 1 : 0;
         int rc = sweep(h, d, p);
         if (rc) return rc;
     }
@@ -467,6 +468,7 @@ int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, doub
         p.want_reduce = (reduce && last) ? 1 : 0;
         p.t = t;
         p.ctl = ctl;
+        p.gravity = (h->cfg.source_type == 1 && last) ? 1 : 0;
         int rc = sweep(h, d, p);
         if (rc) return rc;
     }
@@ -612,6 +614,7 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     // the mixed form reconstructs in FP32 (multi-dimensional fast flavour only);
     // the strict flavour is the bit-for-bit FP64 build
     if (cfg->precision == CFD_PREC_MIXED && (cfg->dim < 2 || cfg->strict)) return CFD_ERR_UNSUPPORTED;
+    if (cfg->source_type != 0 && !(cfg->source_type == 1 && cfg->dim == 2)) return CFD_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) {
         if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
         if (d >= cfg->dim && cfg->n[d] != 1) return CFD_ERR_CONFIG;
@@ -1163,6 +1166,7 @@ SweepParams batch_params(cfd_batch *b, int c, int slot, int stage, int d)
     p.rkC = stage == 1 ? 0.0 : stage == 2 ? 0.25 : 2.0 / 3.0;
     p.want_reduce = (stage == 3 && last) ? 1 : 0;
     p.ctl = b->ctl + c;
+    p.gravity = (h->cfg.source_type == 1 && last) ? 1 : 0;
     return p;
 }
 

@@ -246,6 +246,16 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
                 double r = p.first ? (0.0 + d) : (p.rhs[gi] + d);
+                if constexpr (NV == 4) {
+                    // SourceTerm::calGravitySource (sourceTerm.cpp:3-20) on the
+                    // stage's prim: rhs(rho v) -= rho, rhs(rho E) -= rho v
+                    if (p.gravity) {
+                        const int sc0 = (i - s_begin + 4) % R;
+                        const double rho = sp[(0 * W + tl) * LSP + sc0];
+                        if (v == 2) r -= rho;
+                        if (v == 3) r -= rho * sp[(2 * W + tl) * LSP + sc0];
+                    }
+                }
                 if (p.mode != MODE_RK) {
                     p.rhs[gi] = r;
                 } else {

@@ -70,6 +70,7 @@ struct SweepParams {
     double icst;        // interpolator constant (TENO cutoff)
     int seg_len;        // cells per CTA segment along the sweep
     int prec;           // 0: FP64 reconstruction, 1: mixed FP32/FP64 (fast flavour only)
+    int gravity;        // 1: add the gravity source of the stage's input state (last direction only)
 };
 
 // One batched sweep launch: the parameter blocks of every case (device array)

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import math
 
 import numpy as np
 
@@ -100,6 +101,11 @@ class EquationType(enum.IntEnum):  # macro.hpp:84
     ACCURACYTEST = 3
 
 
+class SourceType(enum.IntEnum):  # macro.hpp:90
+    SOURCENULL = 0
+    GRAVITY = 1
+
+
 class FluxMethod(enum.IntEnum):  # macro.hpp:86
     HLLC = 0
     ROE = 1
@@ -126,6 +132,7 @@ class Info:
         self.diffMethod = DiffMethod.MND6
         self.interMethod = InterMethod.WCNS5
         self.fluxMethod = FluxMethod.ROE
+        self.sourceType = SourceType.SOURCENULL
         self.iMax = [201, 201, 2]
         self.calZone = [0.0, 0.3, 0.0, 0.3, 0.0, 2.0]
         self.constH = True
@@ -195,6 +202,7 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
     cfg.strict = int(bool(info.strict))
     cfg.precision = int(getattr(info, "precision", 0))
     cfg.device = int(info.device)
+    cfg.source_type = int(getattr(info, "sourceType", 0))
     types = bc if bc is not None else default_bc_types(info)
     if periodic:
         types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]
@@ -202,6 +210,43 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
         for s in range(2):
             cfg.bc[d][s] = int(types[d][s])
     return cfg
+
+
+def _set_line_bc(lib, h, nvar, idim, i, j, side, bnd_type, i0=0, offset=0, ghost_prim=None):
+    gp = None
+    if ghost_prim is not None:
+        gp = np.ascontiguousarray(np.broadcast_to(np.asarray(ghost_prim, dtype=np.float64), (4, nvar)))
+    _lib.check(lib.cfd_set_line_bc(h, idim, i, j, side, int(bnd_type), int(i0), int(offset),
+                                   _lib.ptr(gp) if gp is not None else None), h)
+
+
+def wire_case_bnds(lib, h, info: Info):
+    """The per-line boundary wiring Initializer::initBnds gives a named 2D case
+    beyond its per-direction types: the RTI Dirichlet values (nCase 3,
+    initializer.cpp:831-861) and Initializer::initDoubleMachBnds (nCase 4,
+    initializer.cpp:880-943)."""
+    if info.dim != 2 or info.nCase not in (3, 4):
+        return
+    n = info.icMax()
+    nx, ny = n[0], n[1]
+    nv = info.nPrim()
+    if info.nCase == 3:
+        for i in range(nx):
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, [2.0, 0, 0, 1.0])
+            _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DIRICLET, i + (ny - 1) * nx, -nx, [1.0, 0, 0, 2.5])
+        return
+    post = [8.0, 8.25 * math.cos(math.pi / 6), -8.25 * math.sin(math.pi / 6), 116.5]
+    hx = info.geth(0)
+    for j in range(ny):
+        _set_line_bc(lib, h, nv, 1, j, 0, 0, BndType.DIRICLET, j * nx, 1, post)
+        _set_line_bc(lib, h, nv, 1, j, 0, 1, BndType.SUPERSONICOUTLET, j * nx + nx - 1, -1)
+    for i in range(nx):
+        x = info.calZone[0] + (i + 0.5) * hx  # Block::coorCel as initializer.cpp:677 fills it
+        if x < 1.0 / 6.0:
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, post)
+        else:
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.SYMMETRYY, i, nx)
+        _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DoubleMachUp, i + (ny - 1) * nx, -nx)
 
 
 class BlockSolver:
@@ -226,8 +271,8 @@ class BlockSolver:
         if rc != 0:
             raise _lib.CfdError(rc, "cfd_create")
         self.h = h
-        if info.dim == 2 and info.nCase == 3 and bc is None and not periodic:
-            self._wire_rti()
+        if bc is None and not periodic:
+            wire_case_bnds(self.lib, self.h, info)
 
     # --- lifetime
     def close(self):
@@ -245,20 +290,7 @@ class BlockSolver:
     def set_line_bc(self, idim: int, i: int, j: int, side: int, bnd_type: int, i0: int = 0, offset: int = 0,
                     ghost_prim=None):
         """Mirror of OneDBnd::setUpdate/setValue for one line end (idim 1-based)."""
-        gp = None
-        if ghost_prim is not None:
-            gp = np.ascontiguousarray(np.broadcast_to(np.asarray(ghost_prim, dtype=np.float64),
-                                                       (4, self.nvar)))
-        _lib.check(self.lib.cfd_set_line_bc(self.h, idim, i, j, side, int(bnd_type), int(i0), int(offset),
-                                            _lib.ptr(gp) if gp is not None else None), self.h)
-
-    def _wire_rti(self):
-        # initializer.cpp:831-861: Dirichlet y ends with (2,0,0,1) below and (1,0,0,2.5) above
-        nx = self.n[0]
-        ny = self.n[1]
-        for i in range(nx):
-            self.set_line_bc(2, i, 0, 0, BndType.DIRICLET, i, nx, [2.0, 0, 0, 1.0])
-            self.set_line_bc(2, i, 0, 1, BndType.DIRICLET, i + (ny - 1) * nx, -nx, [1.0, 0, 0, 2.5])
+        _set_line_bc(self.lib, self.h, self.nvar, idim, i, j, side, bnd_type, i0, offset, ghost_prim)
 
     # --- state access (reference AoS layout)
     def set_cons(self, cons: np.ndarray):
@@ -364,6 +396,8 @@ class BlockBatch:
             ch = C.c_void_p()
             _lib.check(self.lib.cfd_batch_case(self.h, i, C.byref(ch)))
             self.cases.append(ch)
+            if bc is None and not periodic:
+                wire_case_bnds(self.lib, ch, self.infos[i])
 
     def close(self):
         if getattr(self, "h", None):
@@ -380,6 +414,12 @@ class BlockBatch:
         info = self.infos[i]
         n = info.icMax()
         return n[0] * n[1] * n[2], info.nPrim()
+
+    def set_line_bc(self, case: int, idim: int, i: int, j: int, side: int, bnd_type: int, i0: int = 0,
+                    offset: int = 0, ghost_prim=None):
+        """BlockSolver.set_line_bc on one case of the batch."""
+        _set_line_bc(self.lib, self.cases[case], self._shape(case)[1], idim, i, j, side, bnd_type, i0, offset,
+                     ghost_prim)
 
     def set_cons(self, i, cons):
         nc, nv = self._shape(i)

@@ -86,6 +86,8 @@ typedef struct cfd_config {
                            high side i0 = last cell, offset = -stride (calOffsetInverse) */
     int device;         /* CUDA device ordinal */
     int seg_len[3];     /* cells per CTA segment along each sweep (0 = autotuned default) */
+    int source_type;    /* SourceType (macro.hpp:90): 0 none, 1 GRAVITY (2D; SourceTerm::calGravitySource,
+                           sourceTerm.cpp:3-20: rhs_(rho v) -= rho, rhs_(rho E) -= rho v) */
 } cfd_config;
 
 typedef struct cfd_handle cfd_handle;

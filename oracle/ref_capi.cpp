@@ -64,6 +64,7 @@ struct ref_cfg {
     int flux_method;    // FluxMethod: HLLC=0, ROE=1
     int n_case;         // Info::nCase: selects the initial state and BC wiring
     double cfl;         // Info::CFL
+    int source_type;    // Info::sourceType (0 SOURCENULL, 1 GRAVITY)
 };
 
 struct ref_handle {
@@ -81,6 +82,7 @@ void *ref_create(const ref_cfg *c)
     info->interMethod = (InterMethod)c->inter_method;
     info->nCase = c->n_case;
     info->CFL = c->cfl;
+    info->sourceType = (SourceType)c->source_type;
     info->dim = c->dim;
     for (int i = 0; i < 6; i++) info->calZone[i] = c->zone[i];
     // iMax counts vertices; Info::icMax() gives cells = iMax - 1 (info.cpp:120-129).

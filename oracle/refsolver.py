@@ -19,7 +19,7 @@ REF_LIB = HERE / "_ref" / "libcongfd_ref.so"
 
 class RefCfg(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("zone", C.c_double * 6), ("inter_method", C.c_int),
-                ("flux_method", C.c_int), ("n_case", C.c_int), ("cfl", C.c_double)]
+                ("flux_method", C.c_int), ("n_case", C.c_int), ("cfl", C.c_double), ("source_type", C.c_int)]
 
 
 _lib = None
@@ -81,12 +81,14 @@ class RefSolver:
     line end to a true wrap (PERIODIC1D with i0/offset pointing at the far end).
     """
 
-    def __init__(self, dim, n, zone, inter_method=2, flux_method=0, n_case=0, cfl=0.5, periodic=False, threads=None):
+    def __init__(self, dim, n, zone, inter_method=2, flux_method=0, n_case=0, cfl=0.5, periodic=False, threads=None,
+                 source_type=0):
         self.lib = load()
         if threads is not None:
             self.lib.ref_set_threads(int(threads))
         n3 = list(n) + [1] * (3 - len(n))
-        cfg = RefCfg(dim, (C.c_int * 3)(*n3), (C.c_double * 6)(*zone), inter_method, flux_method, n_case, cfl)
+        cfg = RefCfg(dim, (C.c_int * 3)(*n3), (C.c_double * 6)(*zone), inter_method, flux_method, n_case, cfl,
+                     source_type)
         self.h = self.lib.ref_create(C.byref(cfg))
         self.dim = dim
         self.n = n3
