@@ -228,6 +228,7 @@ def run_ours(args, rank, world, local_rank):
     info.CFL = cfl
     info.device = local_rank
     info.strict = False
+    info.precision = 1 if args.precision == "mixed" else 0
     solver = zone.BlockSolver(info, periodic=True)
     lib = solver.lib
     c, h = initial_state(dim, n, L)
@@ -336,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the mixed FP32/FP64 form on the same workload, and both forms' accuracy
     mixed = None
-    if not args.no_mixed:
+    if not args.no_mixed and args.precision == "fp64":
         info_m = zone.Info()
         for k, v in vars(info).items():
             setattr(info_m, k, v)
@@ -367,7 +368,8 @@ def run_ours(args, rank, world, local_rank):
     result = {
         "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial field of the configuration)",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 state, f32 reconstruction",
+        "data": "synthetic (analytic initial field of the configuration)",
         "config": {"workload": desc, "grid": [n] * dim, "cells": ncell, "inter_method": im,
                    "flux_method": "Roe" if fm else "HLLC", "cfl": cfl, "flavour": "fast (FMA, 1e-12 parity)",
                    "l2": "inputs larger than L2: 3 state arrays + RHS of %.0f MB each" % (state_bytes / 1e6),
@@ -403,6 +405,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="form of the timed steps (mixed: CFD_PREC_MIXED)")
     ap.add_argument("--accuracy-grid", type=int, default=512)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -119,10 +119,10 @@ __global__ void step_end_kernel(cfd::StepCtl *c, const unsigned long long *red, 
 
 // Pointwise test kernels.
 template <int FAM>
-__global__ void eval_inter5_kernel(const double *q, int n, double c, double *out)
+__global__ void eval_inter5_kernel(const double *q, int n, double c, double kap, double *out)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = cfd::inter5<FAM>(q[5 * i], q[5 * i + 1], q[5 * i + 2], q[5 * i + 3], q[5 * i + 4], c);
+    if (i < n) out[i] = cfd::inter5<FAM>(q[5 * i], q[5 * i + 1], q[5 * i + 2], q[5 * i + 3], q[5 * i + 4], c, kap);
 }
 
 template <int NV, int AX, int FLUX>
@@ -156,7 +156,7 @@ __global__ void accuracy_kernel(const double *q, int n, double h, double c, doub
 
 // One face reconstruction per thread from six stencil prims (known-answer hook).
 template <int NV, int AX, int FAM, int PREC>
-__global__ void eval_face_kernel(const double *prims6, int n, double c, double *out)
+__global__ void eval_face_kernel(const double *prims6, int n, double c, double kap, double *out)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -167,12 +167,23 @@ __global__ void eval_face_kernel(const double *prims6, int n, double c, double *
     }
     double fl[NV], fr[NV];
     if constexpr (NV == 3) {
-        cfd::reconstruct_face<NV, AX, FAM>(pr6, cs6, c, fl, fr);
+        cfd::reconstruct_face<NV, AX, FAM>(pr6, cs6, c, kap, fl, fr);
     } else {
         auto cs = [&](int j, int v) { return cs6[j][v]; };
         auto pr = [&](int j, int v) { return pr6[j][v]; };
-        if constexpr (PREC == 1) cfd::reconstruct_face_mixed<NV, AX, FAM>(cs, pr, c, fl, fr);
-        else cfd::reconstruct_face_stream<NV, AX, FAM>(cs, pr, c, fl, fr);
+        if constexpr (PREC == 1) {
+            // the sweep's FP32 hi/lo split of each stencil cell's cons
+            float hi[6][NV], lo[6][NV];
+            for (int j = 0; j < 6; j++)
+                for (int v = 0; v < NV; v++) {
+                    hi[j][v] = (float)cs6[j][v];
+                    lo[j][v] = (float)(cs6[j][v] - (double)hi[j][v]);
+                }
+            auto inc = [&](int j, int v) { return (hi[j][v] - hi[2][v]) + (lo[j][v] - lo[2][v]); };
+            cfd::reconstruct_face_mixed<NV, AX, FAM>(cs, pr, inc, c, kap, fl, fr);
+        } else {
+            cfd::reconstruct_face_stream<NV, AX, FAM>(cs, pr, c, kap, fl, fr);
+        }
     }
     for (int v = 0; v < NV; v++) {
         out[i * 2 * NV + v] = fl[v];
@@ -225,6 +236,7 @@ struct cfd_handle {
     long long stride[3] = {1, 1, 1};
     int fam = 0;
     double icst = 0.0;
+    double icst_k = 0.0;
     bool strict = false;
     cudaStream_t stream = nullptr;
     double *u[3] = {nullptr, nullptr, nullptr};
@@ -416,6 +428,7 @@ SweepParams base_params(cfd_handle *h, int d)
     p.bc_hi = h->d_bchi[d];
     p.bc_vals = h->d_bcvals;
     p.icst = h->icst;
+    p.icst_k = h->icst_k;
     p.seg_len = h->seg_len[d];
     p.prec = h->cfg.precision == CFD_PREC_MIXED ? 1 : 0;
     p.dm_u = h->dm_u;
@@ -632,6 +645,7 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     h->stride[2] = (long long)cfg->n[0] * cfg->n[1];
     h->fam = im.fam;
     h->icst = im.c;
+    h->icst_k = (im.fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(im.c) : 0.0;
     h->strict = cfg->strict != 0;
     h->dm_u = 8.25 * std::cos(M_PI / 6);
     h->dm_v = -8.25 * std::sin(M_PI / 6);
@@ -937,6 +951,7 @@ int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double
 {
     (void)strict;
     InterMap im = map_inter_method(inter_method, 2);
+    const double kap = (im.fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(im.c) : 0.0;
     if (!im.ok) return CFD_ERR_UNSUPPORTED;
     if (n <= 0) return CFD_OK;
     double *dq = nullptr, *dout = nullptr;
@@ -945,11 +960,11 @@ int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double
     cudaMemcpy(dq, q, sizeof(double) * 5 * n, cudaMemcpyHostToDevice);
     int g = (n + 255) / 256;
     switch (im.fam) {
-    case cfd::FAM_WCNS5: eval_inter5_kernel<cfd::FAM_WCNS5><<<g, 256>>>(dq, n, im.c, dout); break;
-    case cfd::FAM_WENOZ: eval_inter5_kernel<cfd::FAM_WENOZ><<<g, 256>>>(dq, n, im.c, dout); break;
-    case cfd::FAM_TENOZ: eval_inter5_kernel<cfd::FAM_TENOZ><<<g, 256>>>(dq, n, im.c, dout); break;
-    case cfd::FAM_TENOCONG: eval_inter5_kernel<cfd::FAM_TENOCONG><<<g, 256>>>(dq, n, im.c, dout); break;
-    default: eval_inter5_kernel<cfd::FAM_MUSCL><<<g, 256>>>(dq, n, im.c, dout); break;
+    case cfd::FAM_WCNS5: eval_inter5_kernel<cfd::FAM_WCNS5><<<g, 256>>>(dq, n, im.c, kap, dout); break;
+    case cfd::FAM_WENOZ: eval_inter5_kernel<cfd::FAM_WENOZ><<<g, 256>>>(dq, n, im.c, kap, dout); break;
+    case cfd::FAM_TENOZ: eval_inter5_kernel<cfd::FAM_TENOZ><<<g, 256>>>(dq, n, im.c, kap, dout); break;
+    case cfd::FAM_TENOCONG: eval_inter5_kernel<cfd::FAM_TENOCONG><<<g, 256>>>(dq, n, im.c, kap, dout); break;
+    default: eval_inter5_kernel<cfd::FAM_MUSCL><<<g, 256>>>(dq, n, im.c, kap, dout); break;
     }
     cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
     cudaFree(dq);
@@ -990,6 +1005,7 @@ extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, c
     if (dim < 1 || dim > 3 || ax < 0 || ax >= dim || (precision != 0 && precision != 1)) return CFD_ERR_CONFIG;
     if (precision == 1 && dim == 1) return CFD_ERR_UNSUPPORTED;
     InterMap im = map_inter_method(inter_method, dim);
+    const double kap = (im.fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(im.c) : 0.0;
     if (!im.ok) return CFD_ERR_UNSUPPORTED;
     if (n <= 0) return CFD_OK;
     int nv = dim + 2;
@@ -1004,8 +1020,8 @@ extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, c
     bool launched = false;
 #define CFD_EFACE(NV, AX, F)                                                                                  \
     if (!launched && nv == NV && ax == AX && im.fam == F) {                                                   \
-        if (precision == 1) eval_face_kernel<NV, AX, F, (NV >= 4 ? 1 : 0)><<<g, 128>>>(din, n, im.c, dout);  \
-        else eval_face_kernel<NV, AX, F, 0><<<g, 128>>>(din, n, im.c, dout);                                  \
+        if (precision == 1) eval_face_kernel<NV, AX, F, (NV >= 4 ? 1 : 0)><<<g, 128>>>(din, n, im.c, kap, dout); \
+        else eval_face_kernel<NV, AX, F, 0><<<g, 128>>>(din, n, im.c, kap, dout);                             \
         launched = true;                                                                                      \
     }
 #define CFD_EFACE_F(F) CFD_EFACE(3, 0, F) CFD_EFACE(4, 0, F) CFD_EFACE(4, 1, F) CFD_EFACE(5, 0, F) \

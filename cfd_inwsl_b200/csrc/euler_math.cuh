@@ -63,9 +63,33 @@ CFD_HD void candidates3(double q0, double q1, double q2, double q3, double q4,
 }
 
 // The eight fixed stencils selected by a TENO flag word (bit k set = stencil k
-// cut off), interScheme.hpp:445-480 (identical in every TENO variant).
+// cut off), interScheme.hpp:445-480 (identical in every TENO variant). On the
+// device the stencil is a row of a coefficient table applied as one 5-term sum,
+// in the reference's term order: every coefficient is exact in binary, a zero
+// coefficient adds an exact zero and a negative one subtracts, so each row
+// rounds exactly like the reference's expression for finite stencil values.
+#if defined(__CUDACC__)
+static __constant__ double kTenoStencil[8][5] = {
+    {3.0 / 128.0, -5.0 / 32.0, 45.0 / 64.0, 15.0 / 32.0, -5.0 / 128.0},
+    {0.0, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0},
+    {0.0, 0.0, 3.0 / 8.0, 3.0 / 4.0, -1.0 / 8.0},
+    {0.0, 0.0, 3.0 / 8.0, 3.0 / 4.0, -1.0 / 8.0},
+    {1.0 / 16.0, -5.0 / 16.0, 15.0 / 16.0, 5.0 / 16.0, 0.0},
+    {0.0, -1.0 / 8.0, 3.0 / 4.0, 3.0 / 8.0, 0.0},
+    {3.0 / 8.0, -5.0 / 4.0, 15.0 / 8.0, 0.0, 0.0},
+    {0.0, 0.0, 1.0, 0.0, 0.0},
+};
+#endif
 CFD_HD double teno_select(unsigned flag, double q0, double q1, double q2, double q3, double q4)
 {
+#if defined(__CUDA_ARCH__)
+    const double *c = kTenoStencil[flag & 7u];
+    double t = c[0] * q0;
+    t = t + c[1] * q1;
+    t = t + c[2] * q2;
+    t = t + c[3] * q3;
+    return t + c[4] * q4;
+#else
     switch (flag) {
     case 0: return 3.0 / 128.0 * q0 - 5.0 / 32.0 * q1 + 45.0 / 64.0 * q2 + 15.0 / 32.0 * q3 - 5.0 / 128.0 * q4;
     case 1: return -1.0 / 16.0 * q1 + 9.0 / 16.0 * q2 + 9.0 / 16.0 * q3 - 1.0 / 16.0 * q4;
@@ -76,6 +100,23 @@ CFD_HD double teno_select(unsigned flag, double q0, double q1, double q2, double
     case 6: return 3.0 / 8.0 * q0 - 5.0 / 4.0 * q1 + 15.0 / 8.0 * q2;
     default: return q2;
     }
+#endif
+}
+
+// TENO-Z keeps all three stencils (flag 0) when
+// min_k m_k >= CT = c sum_k m_k, m_k = (1 + tau/s_k)^6, s_k = beta_k + eps. A
+// sufficient condition without divisions: m_min >= 3.3 c m_max, i.e.
+// t_min / t_max = (s_max + tau) s_min / ((s_min + tau) s_max) >= kappa with
+// kappa = (3.3 c)^(1/6) (teno_kappa). Its 10% margin over the 3c that
+// sum_k m_k <= 3 m_max needs is far above the rounding of either evaluation, so
+// the early answer is the reference's own flag 0, bit for bit.
+inline double teno_kappa(double c) { return c > 0.0 ? ::pow(3.3 * c, 1.0 / 6.0) : 0.0; }
+
+CFD_HD bool teno_z_all_kept(double s0, double s1, double s2, double tau, double kap)
+{
+    const double smin = fmin(s0, fmin(s1, s2)), smax = fmax(s0, fmax(s1, s2));
+    const double lhs = (smax + tau) * smin, rhs = (smin + tau) * smax;
+    return rhs < 1e300 && lhs >= kap * rhs;
 }
 
 // Interpolator families. Each selector entry of the reference maps onto one
@@ -90,7 +131,7 @@ enum InterFamily : int {
 };
 
 template <int FAM>
-CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, double c)
+CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, double c, double kap = 0.0)
 {
     if constexpr (FAM == FAM_WCNS5) {
         // weno5_JSchen: omega_k = gamma_k / (eps + beta_k)^2, eps = 1e-6.
@@ -137,6 +178,8 @@ CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, doub
         double b0, b1, b2;
         smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
         double tau = fabs(b2 - b0), t;
+        if (kap > 0.0 && teno_z_all_kept(b0 + eps, b1 + eps, b2 + eps, tau, kap))
+            return teno_select(0u, q0, q1, q2, q3, q4);
 #if defined(CFD_FAST)
         // fast path: tau/s_k from one reciprocal of s0 s1 s2 (guarded against
         // overflow/underflow of the product)
@@ -530,7 +573,7 @@ CFD_HD void positive_limit_1d(int which, const double *W, double *Wi)
 // Writes the left and right face prim states.
 // ---------------------------------------------------------------------------
 template <int NV, int AX, int FAM>
-CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], double icst,
+CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], double icst, double kap,
                              double *fl, double *fr)
 {
     Eigen<NV, AX> eig(pr6[2], pr6[3]);
@@ -538,8 +581,8 @@ CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], d
     for (int k = 0; k < NV; k++) {
         double q[6];
         for (int j = 0; j < 6; j++) q[j] = eig.project(k, cs6[j]);
-        QL[k] = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst);
-        QR[k] = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst);
+        QL[k] = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst, kap);
+        QR[k] = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst, kap);
     }
     double cl[NV], cr[NV];
     eig.back(QL, cl);
@@ -692,7 +735,7 @@ struct EigenBase {
 
 // cs(j, v): re-derived cons of stencil cell j (0..5), pr(j, v): its prim.
 template <int NV, int AX, int FAM, class CS, class PR>
-CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, double *fl, double *fr)
+CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, double kap, double *fl, double *fr)
 {
     static_assert(NV == 4 || NV == 5, "multi-dimensional form");
     const EigenBase<NV, AX> eb(pr);
@@ -721,15 +764,15 @@ CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, dou
         }
         double QL, QR;
 #if !defined(CFD_ROLL_FIELDS)
-        QL = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst);
-        QR = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst);
+        QL = inter5<FAM>(q[0], q[1], q[2], q[3], q[4], icst, kap);
+        QR = inter5<FAM>(q[5], q[4], q[3], q[2], q[1], icst, kap);
 #else
         // one interpolator body for both states (mirrored stencil on side 1)
 #pragma unroll 1
         for (int side = 0; side < 2; side++) {
             const bool m = side != 0;
             const double r = inter5<FAM>(m ? q[5] : q[0], m ? q[4] : q[1], q[m ? 3 : 2], q[m ? 2 : 3],
-                                         m ? q[1] : q[4], icst);
+                                         m ? q[1] : q[4], icst, kap);
             if (m) QR = r; else QL = r;
         }
 #endif

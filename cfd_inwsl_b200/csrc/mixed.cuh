@@ -1,15 +1,33 @@
-// Mixed FP32/FP64 face reconstruction (cfd_config.precision = CFD_PREC_MIXED).
+// Mixed FP32/FP64 face reconstruction and Roe flux (cfd_config.precision =
+// CFD_PREC_MIXED).
 //
-// The characteristic projection, the five-point interpolations and the back
-// projection run in FP32, the Riemann flux, the MND6 difference, the state and
-// the RK combination stay FP64. FP32 works on increments, not on the values:
-// every stencil value enters as its FP64 difference to the stencil's centre
-// cell (j = 2), which is O(h) in smooth regions, so FP32 rounding is relative
-// to the increment and the rebuilt FP64 face state keeps about seven digits of
-// the increment instead of seven digits of the state. All interpolators are
-// invariant under adding a constant to the stencil (their smoothness measures
-// use differences and their candidate stencils sum to one), so interpolating
-// the increments and adding the centre value back is the same reconstruction.
+// The state, the face values fed to the Riemann solver, the central part of
+// the flux, the MND6 difference and the RK combination stay FP64. FP32 does the
+// work whose rounding the scheme does not see:
+//
+//   * TENO families (flag-selected stencils): the smoothness measures and the
+//     cut-off decision of every characteristic field run in FP32. When one side
+//     of a face selects the same stencil in every field, the characteristic
+//     projection and its inverse cancel (R L = I), so the face value is that
+//     stencil applied to the FP64 cons component by component; otherwise the
+//     FP64 projection is applied with the FP32-selected stencils. Either way the
+//     face value is an FP64 linear combination of FP64 cells: FP32 only decides
+//     which combination, and a decision can differ from the FP64 one only where
+//     a stencil's measure sits within FP32 rounding of the cut-off.
+//   * Continuous-weight families (WCNS5, WENO-Z, MUSCL): the face increment is
+//     split into the component-wise linear interpolation (FP32 on increments,
+//     error relative to the increment) plus the characteristic nonlinear
+//     correction R (NL(L dU) - Lin(L dU)) in FP32.
+//   * Roe flux: the central part (F_L + F_R) / 2 in FP64, the upwind
+//     dissipation R |Lambda| L (U_R - U_L) / 2 in FP32 from FP64 jumps; the
+//     dissipation is O(jump), small wherever the data are smooth.
+//
+// FP32 works on increments, never on the values: every stencil value enters as
+// cons(j) - cons(2), formed from an FP32 hi/lo split of each cell's cons
+// (hi = (float)U, lo = (float)(U - hi)), so neighbouring hi parts subtract
+// exactly and the increment keeps about seven digits of itself. All
+// interpolators are invariant under adding a constant to the stencil (their
+// smoothness measures use differences and their candidate stencils sum to one).
 //
 // FP32 cannot hold the FP64 constants of the TENO family as they are:
 //   * eps = 1e-40 is below FP32's normal range: 1e-30 is used;
@@ -102,6 +120,48 @@ __device__ __forceinline__ float inter5f(float q0, float q1, float q2, float q3,
     }
 }
 
+// The 3-bit cut-off flag of the TENO families in FP32 (bit k set = stencil k
+// cut), the decision of inter5<FAM_TENOZ / FAM_TENOCONG> in euler_math.cuh.
+template <int FAM>
+__device__ __forceinline__ unsigned teno_flag_f(float q0, float q1, float q2, float q3, float q4, float c, float kap)
+{
+    float b0, b1, b2;
+    {
+        float a = q0 - 2.0f * q1 + q2, b = q0 - 4.0f * q1 + 3.0f * q2;
+        b0 = a * a + 0.25f * (b * b);
+        a = q1 - 2.0f * q2 + q3;
+        b = q1 - q3;
+        b1 = a * a + 0.25f * (b * b);
+        a = q2 - 2.0f * q3 + q4;
+        b = 3.0f * q2 - 4.0f * q3 + q4;
+        b2 = a * a + 0.25f * (b * b);
+    }
+    const float tau = fabsf(b2 - b0);
+    if constexpr (FAM == FAM_TENOZ) {
+        {
+            // the keep-all bound of teno_z_all_kept (euler_math.cuh)
+            const float s0 = b0 + 1e-30f, s1 = b1 + 1e-30f, s2 = b2 + 1e-30f;
+            const float smin = fminf(s0, fminf(s1, s2)), smax = fmaxf(s0, fmaxf(s1, s2));
+            const float rhs = (smin + tau) * smax;
+            if (rhs < 1e36f && (smax + tau) * smin >= kap * rhs) return 0u;
+        }
+        float t0 = 1.0f + __fdividef(tau, b0 + 1e-30f), t1 = 1.0f + __fdividef(tau, b1 + 1e-30f),
+              t2 = 1.0f + __fdividef(tau, b2 + 1e-30f);
+        const float itm = __fdividef(1.0f, fmaxf(t0, fmaxf(t1, t2)));
+        t0 *= itm; t1 *= itm; t2 *= itm;
+        float m0 = t0 * t0, m1 = t1 * t1, m2 = t2 * t2;
+        m0 = m0 * m0 * m0; m1 = m1 * m1 * m1; m2 = m2 * m2 * m2;
+        const float CT = c * (m0 + m1 + m2);
+        return (m0 < CT ? 1u : 0u) + (m1 < CT ? 2u : 0u) + (m2 < CT ? 4u : 0u);
+    } else {
+        float bmin = b0;
+        if (b1 < bmin) bmin = b1;
+        if (b2 < bmin) bmin = b2;
+        const float rr = c * tau - (1.0f - c) * bmin, ll = tau * bmin;
+        return (ll < rr * b0 ? 1u : 0u) + (ll < rr * b1 ? 2u : 0u) + (ll < rr * b2 ? 4u : 0u);
+    }
+}
+
 // Roe-averaged eigenvectors in FP32 from the FP64 base quantities.
 template <int NV, int AX>
 struct EigenF {
@@ -117,10 +177,10 @@ struct EigenF {
         float kl = (float)(vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]);
         float kr = (float)(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
         const float g1 = (float)(kGamma / (kGamma - 1));
-        float HL = 0.5f * kl + (float)pL * (g1 / (float)rl);
-        float HR = 0.5f * kr + (float)pR * (g1 / (float)rr);
+        float HL = 0.5f * kl + (float)pL * __fdividef(g1, (float)rl);
+        float HR = 0.5f * kr + (float)pR * __fdividef(g1, (float)rr);
         float c1 = sqrtf((float)rl), c2 = sqrtf((float)rr);
-        float dv = 1.0f / (c1 + c2);
+        float dv = __fdividef(1.0f, c1 + c2);
         u = (c1 * (float)vl[0] + c2 * (float)vr[0]) * dv;
         v = (c1 * (float)vl[1] + c2 * (float)vr[1]) * dv;
         w = (c1 * (float)vl[2] + c2 * (float)vr[2]) * dv;
@@ -129,8 +189,8 @@ struct EigenF {
         ek = 0.5f * (u * u + v * v + w * w);
         h = ht - ek;
         c = sqrtf((float)(kGamma - 1) * h);
-        ic = 1.0f / c;
-        ih = 1.0f / h;
+        ic = __fdividef(1.0f, c);
+        ih = __fdividef(1.0f, h);
     }
     __device__ __forceinline__ float L(int k, int m) const
     {
@@ -179,63 +239,128 @@ __device__ __forceinline__ float lin5f(float q0, float q1, float q2, float q3, f
     return 0.0234375f * q0 - 0.15625f * q1 + 0.703125f * q2 + 0.46875f * q3 - 0.0390625f * q4;
 }
 
-// cs(j, v) / pr(j, v): FP64 cons and prim of stencil cell j; writes FP64 face prims.
+// FP64 face states from per-field stencil flags: the characteristic projection
+// of reconstruct_face_stream (euler_math.cuh) with the interpolation replaced
+// by the selected fixed stencil. fL/fR hold 3 bits per field.
+template <int NV, int AX, class CS, class PR>
+__device__ __noinline__ void recon_flags64(const CS &cs, const PR &pr, unsigned fL, unsigned fR, double *cl,
+                                           double *cr)
+{
+    const EigenBase<NV, AX> eb(pr);
+#pragma unroll
+    for (int i = 0; i < NV; i++) cl[i] = cr[i] = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < NV; k++) {
+        double l[NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
+        double q[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            double a = cs(j, 1) * l[1] + cs(j, 2) * l[2];
+#pragma unroll
+            for (int m = 3; m < NV; m++) a = a + cs(j, m) * l[m];
+            q[j] = a + cs(j, 0) * l[0];
+        }
+        const double QL = teno_select((fL >> (3 * k)) & 7u, q[0], q[1], q[2], q[3], q[4]);
+        const double QR = teno_select((fR >> (3 * k)) & 7u, q[5], q[4], q[3], q[2], q[1]);
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            const double r = eb.R(i, k);
+            cl[i] = cl[i] + QL * r;
+            cr[i] = cr[i] + QR * r;
+        }
+    }
+}
+
+// cs(j, v) / pr(j, v): FP64 cons and prim of stencil cell j; inc(j, v): FP32
+// cons(j, v) - cons(2, v). Writes FP64 face prims.
 //
-// The face increment is split as U_face - U_2 = Lin(dU) + R (NL(q) - Lin(q)),
-// q = L dU, which equals R NL(L dU) in exact arithmetic because the linear
-// interpolation commutes with the projection. The linear part is interpolated
-// component by component, so its FP32 error is relative to dU itself; only the
-// nonlinear correction passes through the FP32 eigenvectors, whose R L differs
-// from the identity by about 1e-7 times their condition number (large at low
-// Mach number, where h = c^2/(gamma-1) dominates). The correction vanishes
-// where the scheme is linear (TENO with every stencil kept) and is small
-// wherever the data are smooth.
-template <int NV, int AX, int FAM, class CS, class PR>
-__device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &pr, double icst, double *fl,
-                                                       double *fr)
+// Continuous-weight families: the face increment is split as
+// U_face - U_2 = Lin(dU) + R (NL(q) - Lin(q)), q = L dU, which equals
+// R NL(L dU) in exact arithmetic because the linear interpolation commutes with
+// the projection. The linear part is interpolated component by component, so
+// its FP32 error is relative to dU itself; only the nonlinear correction passes
+// through the FP32 eigenvectors, whose R L differs from the identity by about
+// 1e-7 times their condition number (large at low Mach number, where
+// h = c^2/(gamma-1) dominates).
+template <int NV, int AX, int FAM, class CS, class PR, class INC>
+__device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &pr, const INC &inc, double icst,
+                                                       double kap, double *fl, double *fr)
 {
     const EigenF<NV, AX> eb(pr);
-    // increments of the stencil cons relative to cell 2, in FP32
     float d[6][NV];
 #pragma unroll
     for (int j = 0; j < 6; j++)
 #pragma unroll
-        for (int m = 0; m < NV; m++) d[j][m] = (j == 2) ? 0.0f : (float)(cs(j, m) - cs(2, m));
-    float dl[NV], dr[NV];
+        for (int m = 0; m < NV; m++) d[j][m] = (j == 2) ? 0.0f : inc(j, m);
+    const float fc = (float)icst, fk = (float)kap;
+    double cl[NV], cr[NV];
+    if constexpr (FAM == FAM_TENOZ || FAM == FAM_TENOCONG) {
+        unsigned fL = 0, fR = 0;
 #pragma unroll
-    for (int i = 0; i < NV; i++) {
-        dl[i] = lin5f(d[0][i], d[1][i], d[2][i], d[3][i], d[4][i]);
-        dr[i] = lin5f(d[5][i], d[4][i], d[3][i], d[2][i], d[1][i]);
-    }
-    const float fc = (float)icst;
+        for (int k = 0; k < NV; k++) {
+            float l[NV];
 #pragma unroll
-    for (int k = 0; k < NV; k++) {
-        float l[NV];
+            for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
+            float q[6];
 #pragma unroll
-        for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
-        float q[6];
+            for (int j = 0; j < 6; j++) {
+                float a = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 6; j++) {
-            float a = 0.0f;
-#pragma unroll
-            for (int m = 0; m < NV; m++) a += d[j][m] * l[m];
-            q[j] = a;
+                for (int m = 0; m < NV; m++) a += d[j][m] * l[m];
+                q[j] = a;
+            }
+            fL |= teno_flag_f<FAM>(q[0], q[1], q[2], q[3], q[4], fc, fk) << (3 * k);
+            fR |= teno_flag_f<FAM>(q[5], q[4], q[3], q[2], q[1], fc, fk) << (3 * k);
         }
-        const float CL = inter5f<FAM>(q[0], q[1], q[2], q[3], q[4], fc) - lin5f(q[0], q[1], q[2], q[3], q[4]);
-        const float CR = inter5f<FAM>(q[5], q[4], q[3], q[2], q[1], fc) - lin5f(q[5], q[4], q[3], q[2], q[1]);
+        // one stencil in every field: R L = I, apply it to the cons directly
+        constexpr unsigned kRep = (NV == 4) ? 01111u : 011111u;
+        const unsigned sL = fL & 7u, sR = fR & 7u;
+        if (fL == sL * kRep && fR == sR * kRep) {
+#pragma unroll
+            for (int m = 0; m < NV; m++) {
+                cl[m] = teno_select(sL, cs(0, m), cs(1, m), cs(2, m), cs(3, m), cs(4, m));
+                cr[m] = teno_select(sR, cs(5, m), cs(4, m), cs(3, m), cs(2, m), cs(1, m));
+            }
+        } else {
+            recon_flags64<NV, AX>(cs, pr, fL, fR, cl, cr);
+        }
+    } else {
+        float dl[NV], dr[NV];
 #pragma unroll
         for (int i = 0; i < NV; i++) {
-            const float r = eb.R(i, k);
-            dl[i] += CL * r;
-            dr[i] += CR * r;
+            dl[i] = lin5f(d[0][i], d[1][i], d[2][i], d[3][i], d[4][i]);
+            dr[i] = lin5f(d[5][i], d[4][i], d[3][i], d[2][i], d[1][i]);
         }
-    }
-    double cl[NV], cr[NV];
 #pragma unroll
-    for (int i = 0; i < NV; i++) {
-        const double base = cs(2, i);
-        cl[i] = base + (double)dl[i];
-        cr[i] = base + (double)dr[i];
+        for (int k = 0; k < NV; k++) {
+            float l[NV];
+#pragma unroll
+            for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
+            float q[6];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                float a = 0.0f;
+#pragma unroll
+                for (int m = 0; m < NV; m++) a += d[j][m] * l[m];
+                q[j] = a;
+            }
+            const float CL = inter5f<FAM>(q[0], q[1], q[2], q[3], q[4], fc) - lin5f(q[0], q[1], q[2], q[3], q[4]);
+            const float CR = inter5f<FAM>(q[5], q[4], q[3], q[2], q[1], fc) - lin5f(q[5], q[4], q[3], q[2], q[1]);
+#pragma unroll
+            for (int i = 0; i < NV; i++) {
+                const float r = eb.R(i, k);
+                dl[i] += CL * r;
+                dr[i] += CR * r;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            const double base = cs(2, i);
+            cl[i] = base + (double)dl[i];
+            cr[i] = base + (double)dr[i];
+        }
     }
     char_cons_to_prim<NV>(cl, fl);
     char_cons_to_prim<NV>(cr, fr);
@@ -247,6 +372,77 @@ __device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &p
         for (int i = 1; i < NV - 1; i++) fr[i] = pr(2, i);
         fr[NV - 1] = pr(3, NV - 1);
     }
+}
+
+// roeFlux2DSym (fluxSchemes.hpp:420-553) and its 3D extension with the central
+// part in FP64 and the dissipation in FP32. rho H = rho |v|^2 / 2 + gamma p /
+// (gamma - 1) needs no division in the central part.
+template <int NV, int AX>
+__device__ __forceinline__ void roe_md_mixed(const double *L, const double *R, double *res)
+{
+    constexpr int D = NV - 2, E = NV - 1;
+    const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+    const double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
+    const double *vl = L + 1, *vr = R + 1;
+    double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+    if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+    const double VnL = vl[AX], VnR = vr[AX];
+    constexpr double kg1 = kGamma / (kGamma - 1);
+    double Fc[NV];
+    Fc[0] = rl * VnL + rr * VnR;
+#pragma unroll
+    for (int i = 0; i < D; i++) Fc[1 + i] = rl * vl[i] * VnL + rr * vr[i] * VnR + (pl + pr) * n[i];
+    Fc[E] = (0.5 * rl * kl + kg1 * pl) * VnL + (0.5 * rr * kr + kg1 * pr) * VnR;
+
+    // jumps in FP64, then FP32
+    const float dP = (float)(pr - pl), dVn = (float)(VnR - VnL), dRho = (float)(rr - rl);
+    float dv[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int i = 0; i < D; i++) dv[i] = (float)(vr[i] - vl[i]);
+    const float rlf = (float)rl, rrf = (float)rr;
+    float vlf[3], vrf[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        vlf[i] = i < D ? (float)vl[i] : 0.0f;
+        vrf[i] = i < D ? (float)vr[i] : 0.0f;
+    }
+    const float g1 = (float)kg1;
+    const float HL = 0.5f * (float)kl + (float)pl * __fdividef(g1, rlf);
+    const float HR = 0.5f * (float)kr + (float)pr * __fdividef(g1, rrf);
+    const float c1 = sqrtf(rlf), c2 = sqrtf(rrf);
+    const float dvs = __fdividef(1.0f, c1 + c2);
+    const float rhoAvg = c1 * c2;
+    float vAvg[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) vAvg[i] = (c1 * vlf[i] + c2 * vrf[i]) * dvs;
+    const float HAvg = (c1 * HL + c2 * HR) * dvs;
+    const float q2 = 0.5f * (vAvg[0] * vAvg[0] + vAvg[1] * vAvg[1] + vAvg[2] * vAvg[2]);
+    const float cAvg = sqrtf((float)(kGamma - 1) * (HAvg - q2));
+    const float VnAvg = vAvg[AX];
+    float lam[3] = {fabsf(VnAvg - cAvg), fabsf(VnAvg), fabsf(VnAvg + cAvg)};
+    const float eps = 0.05f * (fabsf(VnAvg) + cAvg);
+    const float ie2 = __fdividef(0.5f, eps);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        if (lam[i] < eps) lam[i] = (lam[i] * lam[i] + eps * eps) * ie2;
+    const float ic2 = __fdividef(1.0f, cAvg * cAvg);
+    const float a1 = lam[0] * ((dP - rhoAvg * cAvg * dVn) * (0.5f * ic2));
+    const float a3 = lam[2] * ((dP + rhoAvg * cAvg * dVn) * (0.5f * ic2));
+    const float a2 = lam[1] * (dRho - dP * ic2);
+    const float l1r = lam[1] * rhoAvg;
+    float Fd[NV];
+    Fd[0] = a1 + a3 + a2;
+    float tE = 0.0f;
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+        const float ni = (i == AX) ? 1.0f : 0.0f;
+        const float ti = (i == AX) ? 0.0f : dv[i];
+        Fd[1 + i] = a1 * (vAvg[i] - cAvg * ni) + a3 * (vAvg[i] + cAvg * ni) + a2 * vAvg[i] + l1r * ti;
+        if (i != AX) tE += vAvg[i] * dv[i];
+    }
+    Fd[E] = a1 * (HAvg - cAvg * VnAvg) + a3 * (HAvg + cAvg * VnAvg) + a2 * q2 + l1r * tE;
+#pragma unroll
+    for (int i = 0; i < NV; i++) res[i] = 0.5 * (Fc[i] - (double)Fd[i]);
 }
 
 } // namespace cfd

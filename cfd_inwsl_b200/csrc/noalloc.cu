@@ -10,6 +10,7 @@
 //
 // Compiled with --fmad=false like api.cu.
 #include "cfdgpu.h"
+#include "euler_math.cuh"
 #include "sweep_dispatch.h"
 
 #include <cstdio>
@@ -183,6 +184,7 @@ extern "C" int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, do
         p.bc_vals = nullptr;
         p.t = t;
         p.icst = icst;
+        p.icst_k = (fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(icst) : 0.0;
         p.seg_len = cfg->seg_len[d] > 0 ? cfg->seg_len[d] : cfg->n[d];
         p.dm_u = 8.25 * std::cos(M_PI / 6);
         p.dm_v = -8.25 * std::sin(M_PI / 6);

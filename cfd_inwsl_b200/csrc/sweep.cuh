@@ -87,15 +87,25 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     }
 }
 
+constexpr int pow2_ceil(int x)
+{
+    int r = 1;
+    while (r < x) r <<= 1;
+    return r;
+}
+
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC = 0>
 struct SweepShape {
     static constexpr int NT = S * W;
-    static constexpr int R = S + 8;           // prim ring positions
-    static constexpr int RF = S + 3;          // face ring positions
+    // ring sizes are powers of two so that ring positions are bit masks
+    static constexpr int R = pow2_ceil(S + 8);   // prim ring positions (S + 8 used)
+    static constexpr int RF = pow2_ceil(S + 3);  // face ring positions (S + 3 used)
     static constexpr int LSP = R | 1;         // odd line strides avoid bank conflicts
     static constexpr int LSF = RF | 1;
     static constexpr int SMEM_DOUBLES = 2 * NV * W * LSP + NV * W * LSF;
-    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+    // mixed form: FP32 hi/lo split of the cons ring (exact FP32 increments)
+    static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
 };
 
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
@@ -104,17 +114,22 @@ template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
 #endif
 __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 {
-    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC>;
     constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
     // device-resident loop: the whole launch is a no-op once the loop is done
     if (p.ctl && p.ctl->done) return;
     const double tstage = p.ctl ? p.ctl->tst[p.rk_stage] : p.t;
     const double inv_h = 1.0 / p.h;
+    // ring positions (R and RF are powers of two; arguments are never negative)
+    auto ring = [](int x) { return (int)((unsigned)x & (unsigned)(R - 1)); };
+    auto fring = [](int x) { return (int)((unsigned)x & (unsigned)(RF - 1)); };
     const double rkBdt = p.ctl ? p.ctl->bdt[p.rk_stage] : p.rkBdt;
     extern __shared__ double smem[];
     double *sp = smem;                   // [NV][W][LSP] prim
     double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue)
     double *sf = sc + NV * W * LSP;      // [NV][W][LSF] face flux
+    float *shi = reinterpret_cast<float *>(sf + NV * W * LSF);  // mixed form: [NV][W][LSP] (float)cons
+    float *slo = shi + NV * W * LSP;                            //             [NV][W][LSP] cons - hi
 
     constexpr int T0 = (AX == 0) ? 1 : 0;  // transverse axis with neighbouring lines in a CTA
     constexpr int T1 = (AX == 2) ? 1 : 2;
@@ -162,11 +177,16 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         }
         double cs[NV];
         prim_to_cons<NV>(pr, cs);
-        int slot = (P - s_begin + 4) % R;
+        int slot = ring(P - s_begin + 4);
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             sp[(v * W + l) * LSP + slot] = pr[v];
             sc[(v * W + l) * LSP + slot] = cs[v];
+            if constexpr (PREC == 1) {
+                const float hi = (float)cs[v];
+                shi[(v * W + l) * LSP + slot] = hi;
+                slo[(v * W + l) * LSP + slot] = (float)(cs[v] - (double)hi);
+            }
         }
     };
 
@@ -174,7 +194,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     auto face = [&](int l, int j) {
         int slot[6];
 #pragma unroll
-        for (int m = 0; m < 6; m++) slot[m] = (j - 3 + m - s_begin + 4) % R;
+        for (int m = 0; m < 6; m++) slot[m] = ring(j - 3 + m - s_begin + 4);
         double fl[NV], fr[NV], fx[NV];
         if constexpr (NV == 3) {
             double pr6[6][NV], cs6[6][NV];
@@ -186,16 +206,27 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                     cs6[m][v] = sc[(v * W + l) * LSP + slot[m]];
                 }
             }
-            reconstruct_face<NV, AX, FAM>(pr6, cs6, p.icst, fl, fr);
+            reconstruct_face<NV, AX, FAM>(pr6, cs6, p.icst, p.icst_k, fl, fr);
         } else {
             const double *spl = sp + l * LSP, *scl = sc + l * LSP;
             auto csacc = [&](int m, int v) { return scl[v * W * LSP + slot[m]]; };
             auto pracc = [&](int m, int v) { return spl[v * W * LSP + slot[m]]; };
-            if constexpr (PREC == 1) reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, p.icst, fl, fr);
-            else reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, fl, fr);
+            if constexpr (PREC == 1) {
+                const float *hil = shi + l * LSP, *lol = slo + l * LSP;
+                // cons(j) - cons(2) in FP32: the hi parts of neighbouring cells
+                // subtract exactly wherever the increment is small
+                auto incacc = [&](int m, int v) {
+                    const int a = v * W * LSP;
+                    return (hil[a + slot[m]] - hil[a + slot[2]]) + (lol[a + slot[m]] - lol[a + slot[2]]);
+                };
+                reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, incacc, p.icst, p.icst_k, fl, fr);
+            } else {
+                reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, p.icst_k, fl, fr);
+            }
         }
-        riemann<NV, AX, FLUX>(fl, fr, fx);
-        int fslot = (j - s_begin + 1) % RF;
+        if constexpr (PREC == 1 && FLUX == FLUX_ROE && NV >= 4) roe_md_mixed<NV, AX>(fl, fr, fx);
+        else riemann<NV, AX, FLUX>(fl, fr, fx);
+        int fslot = fring(j - s_begin + 1);
 #pragma unroll
         for (int v = 0; v < NV; v++) sf[(v * W + l) * LSF + fslot] = fx[v];
     };
@@ -228,7 +259,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         line_of(tl, ok, base, lid);
         if (ok && i < s_end) {
             double pm[NV], pp[NV], fnm[NV], fnp[NV];
-            int sm = (i - 1 - s_begin + 4) % R, spp = (i + 1 - s_begin + 4) % R;
+            int sm = ring(i - 1 - s_begin + 4), spp = ring(i + 1 - s_begin + 4);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 pm[v] = sp[(v * W + tl) * LSP + sm];
@@ -236,8 +267,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             }
             node_flux<NV, AX>(pm, fnm);
             node_flux<NV, AX>(pp, fnp);
-            int f0 = (i - 1 - s_begin + 1) % RF, f1 = (i - s_begin + 1) % RF, f2 = (i + 1 - s_begin + 1) % RF,
-                f3 = (i + 2 - s_begin + 1) % RF;
+            int f0 = fring(i - 1 - s_begin + 1), f1 = fring(i - s_begin + 1), f2 = fring(i + 1 - s_begin + 1),
+                f3 = fring(i + 2 - s_begin + 1);
             const long long cell = base + (long long)i * sAX;
             double uo[NV];
 #pragma unroll
@@ -250,7 +281,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                     // SourceTerm::calGravitySource (sourceTerm.cpp:3-20) on the
                     // stage's prim: rhs(rho v) -= rho, rhs(rho E) -= rho v
                     if (p.gravity) {
-                        const int sc0 = (i - s_begin + 4) % R;
+                        const int sc0 = ring(i - s_begin + 4);
                         const double rho = sp[(0 * W + tl) * LSP + sc0];
                         if (v == 2) r -= rho;
                         if (v == 3) r -= rho * sp[(2 * W + tl) * LSP + sc0];
@@ -349,7 +380,7 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
 static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
 {
-    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC>;
     auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC>;
     // the dynamic shared-memory opt-in is per device
     static bool attr_set[64] = {};
@@ -375,7 +406,7 @@ static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
 static cudaError_t launch_batched_shape_p(const BatchSweep &b, cudaStream_t st)
 {
-    using SH = SweepShape<NV, AX, FAM, FLUX, S, W>;
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC>;
     auto kern = sweep_batched_kernel<NV, AX, FAM, FLUX, S, W, PREC>;
     static bool attr_set[64] = {};
     static int blocks_per_sm[64] = {};

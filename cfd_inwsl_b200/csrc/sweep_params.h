@@ -68,6 +68,7 @@ struct SweepParams {
     const StepCtl *ctl; // device-resident step control (null: use rkBdt/t)
     double dm_u, dm_v;  // DoubleMachUp post-shock velocity, 8.25 cos(pi/6) and -8.25 sin(pi/6) from the host libm
     double icst;        // interpolator constant (TENO cutoff)
+    double icst_k;      // TENO-Z early keep-all bound (teno_kappa(icst)); 0 disables it
     int seg_len;        // cells per CTA segment along the sweep
     int prec;           // 0: FP64 reconstruction, 1: mixed FP32/FP64 (fast flavour only)
     int gravity;        // 1: add the gravity source of the stage's input state (last direction only)
