@@ -639,15 +639,33 @@ struct EigenBase {
         double vl[3] = {pr(2, 1), pr(2, 2), D == 3 ? pr(2, 3) : 0.0};
         double vr[3] = {pr(3, 1), pr(3, 2), D == 3 ? pr(3, 3) : 0.0};
         double rl = pr(2, 0), rr = pr(3, 0), pL = pr(2, NV - 1), pR = pr(3, NV - 1);
-        double HL, HR;
 #if defined(CFD_FAST)
-        {
-            double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
-            if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
-            HL = 0.5 * kl + pL * (kG1 / rl);
-            HR = 0.5 * kr + pR * (kG1 / rr);
+        // reciprocal square roots replace the divisions: sqrt(rho) = rho rsqrt(rho),
+        // sqrt(rho) H = sqrt(rho) |v|^2 / 2 + gamma/(gamma-1) p rsqrt(rho),
+        // 1/c = rsqrt(c^2), 1/h = (gamma - 1) / c^2
+        double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+        if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+        const double ir1 = rsqrt(rl), ir2 = rsqrt(rr);
+        const double coef1 = rl * ir1, coef2 = rr * ir2;
+        const double divisor = 1.0 / (coef1 + coef2);
+        u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
+        v = (coef1 * vl[1] + coef2 * vr[1]) * divisor;
+        w = (D == 3) ? (coef1 * vl[2] + coef2 * vr[2]) * divisor : 0.0;
+        const double ht = (0.5 * (coef1 * kl + coef2 * kr) + kG1 * (pL * ir1 + pR * ir2)) * divisor;
+        if constexpr (D == 2) {
+            Vn = nx * u + ny * v;
+            ek = (u * u + v * v) / 2;
+        } else {
+            Vn = nx * u + ny * v + nz * w;
+            ek = (u * u + v * v + w * w) / 2;
         }
+        h = ht - ek;
+        const double c2 = (gamma - 1) * h;
+        ic = rsqrt(c2);
+        c = c2 * ic;
+        ih = (gamma - 1) * (ic * ic);
 #else
+        double HL, HR;
         if constexpr (D == 2) {
             HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pL / rl * gamma / (gamma - 1);
             HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pR / rr * gamma / (gamma - 1);
@@ -655,7 +673,6 @@ struct EigenBase {
             HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pL / rl * gamma / (gamma - 1);
             HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pR / rr * gamma / (gamma - 1);
         }
-#endif
         double coef1 = sqrt(rl), coef2 = sqrt(rr);
         double divisor = 1.0 / (coef1 + coef2);
         u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
@@ -671,9 +688,6 @@ struct EigenBase {
         }
         h = ht - ek;
         c = sqrt((gamma - 1) * h);
-#if defined(CFD_FAST)
-        ic = 1.0 / c;
-        ih = 1.0 / h;
 #endif
     }
 #if defined(CFD_FAST)
@@ -950,24 +964,79 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
     }
 }
 
+#if defined(CFD_FAST)
+// roeFlux2DSym with reciprocal square roots instead of its divisions and square
+// roots: sqrt(rho) = rho rsqrt(rho), sqrt(rho) H = sqrt(rho) |v|^2 / 2 +
+// gamma/(gamma-1) p rsqrt(rho), rho H = rho |v|^2 / 2 + gamma/(gamma-1) p,
+// 1/c = rsqrt(c^2); the entropy fix's 1/(2 eps) only where a wave needs it.
+template <int NV, int AX>
+CFD_HD void roe_md_fast(const double *L, const double *R, double *res)
+{
+    constexpr int D = NV - 2, E = NV - 1;
+    const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+    const double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
+    const double *vl = L + 1, *vr = R + 1;
+    double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+    if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+    const double VnL = vl[AX], VnR = vr[AX];
+    double Fc[NV];
+    Fc[0] = rl * VnL + rr * VnR;
+    for (int i = 0; i < D; i++) Fc[1 + i] = rl * vl[i] * VnL + rr * vr[i] * VnR + (pl + pr) * n[i];
+    Fc[E] = (0.5 * rl * kl + kG1 * pl) * VnL + (0.5 * rr * kr + kG1 * pr) * VnR;
+
+    const double ir1 = rsqrt(rl), ir2 = rsqrt(rr);
+    const double coef1 = rl * ir1, coef2 = rr * ir2;
+    const double divisor = 1.0 / (coef1 + coef2);
+    const double rhoAvg = coef1 * coef2;
+    double vAvg[3];
+    for (int i = 0; i < D; i++) vAvg[i] = (coef1 * vl[i] + coef2 * vr[i]) * divisor;
+    const double HAvg = (0.5 * (coef1 * kl + coef2 * kr) + kG1 * (pl * ir1 + pr * ir2)) * divisor;
+    double q_2Avg;
+    if constexpr (D == 2) q_2Avg = (vAvg[0] * vAvg[0] + vAvg[1] * vAvg[1]) / 2;
+    else q_2Avg = (vAvg[0] * vAvg[0] + vAvg[1] * vAvg[1] + vAvg[2] * vAvg[2]) / 2;
+    const double c2 = (kGamma - 1) * (HAvg - q_2Avg);
+    const double ic = rsqrt(c2);
+    const double cAvg = c2 * ic, ic2 = ic * ic;
+    const double VnAvg = vAvg[AX];
+    double lambda[3] = {fabs(VnAvg - cAvg), fabs(VnAvg), fabs(VnAvg + cAvg)};
+    const double eps = 0.05 * (fabs(VnAvg) + cAvg);
+    if (lambda[0] < eps || lambda[1] < eps || lambda[2] < eps) {
+        const double ie2 = 0.5 / eps;
+        for (int i = 0; i < 3; i++)
+            if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) * ie2;
+    }
+    const double deltaP = pr - pl, deltaVn = VnR - VnL, deltaRho = rr - rl;
+    const double rc = rhoAvg * cAvg * deltaVn;
+    const double a1 = lambda[0] * ((deltaP - rc) * (0.5 * ic2));
+    const double a3 = lambda[2] * ((deltaP + rc) * (0.5 * ic2));
+    const double a2 = lambda[1] * (deltaRho - deltaP * ic2);
+    const double l1r = lambda[1] * rhoAvg;
+    double Fd[NV];
+    Fd[0] = a1 + a3 + a2;
+    double tE = 0.0;
+    for (int i = 0; i < D; i++) {
+        const double ti = (i == AX) ? 0.0 : vr[i] - vl[i];
+        Fd[1 + i] = a1 * (vAvg[i] - cAvg * n[i]) + a3 * (vAvg[i] + cAvg * n[i]) + a2 * vAvg[i] + l1r * ti;
+        if (i != AX) tE += vAvg[i] * ti;
+    }
+    Fd[E] = a1 * (HAvg - cAvg * VnAvg) + a3 * (HAvg + cAvg * VnAvg) + a2 * q_2Avg + l1r * tE;
+    for (int i = 0; i < NV; i++) res[i] = 0.5 * (Fc[i] - Fd[i]);
+}
+#endif
+
 // roeFlux2DSym (fluxSchemes.hpp:420-553), 3D form with both tangential
 // components in the linear wave.
 template <int NV, int AX>
 CFD_HD void roe_md(const double *L, const double *R, double *res)
 {
+#if defined(CFD_FAST)
+    roe_md_fast<NV, AX>(L, R, res);
+#else
     constexpr int D = NV - 2, E = NV - 1;
     const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
     double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
     const double *vl = L + 1, *vr = R + 1;
     double HL, HR;
-#if defined(CFD_FAST)
-    {
-        double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
-        if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
-        HL = 0.5 * kl + pl * (kG1 / rl);
-        HR = 0.5 * kr + pr * (kG1 / rr);
-    }
-#else
     if constexpr (D == 2) {
         HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
         HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
@@ -975,7 +1044,6 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
         HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
         HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
     }
-#endif
     double VnL = vl[AX], VnR = vr[AX];
     double FcL[NV], FcR[NV];
     FcL[0] = rl * VnL;
@@ -998,45 +1066,24 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double VnAvg = vAvg[AX];
     double lambda[3] = {fabs(VnAvg - cAvg), fabs(VnAvg), fabs(VnAvg + cAvg)};
     double eps = 0.05 * (fabs(VnAvg) + cAvg);
-#if defined(CFD_FAST)
-    {
-        const double ie2 = 0.5 / eps;
-        for (int i = 0; i < 3; i++)
-            if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) * ie2;
-    }
-    const double ic2 = 1.0 / (cAvg * cAvg);
-#else
     for (int i = 0; i < 3; i++)
         if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) / (2.0 * eps);
-#endif
 
     double deltaP = pr - pl, deltaVn = VnR - VnL, deltaRho = rr - rl;
     double dv[3];
     for (int i = 0; i < D; i++) dv[i] = vr[i] - vl[i];
     double Fd[NV];
-#if defined(CFD_FAST)
-    double c1 = (deltaP - rhoAvg * cAvg * deltaVn) * (0.5 * ic2);
-#else
     double c1 = (deltaP - rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
-#endif
     Fd[0] = lambda[0] * (c1 * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] = lambda[0] * (c1 * (vAvg[i] - cAvg * n[i]));
     Fd[E] = lambda[0] * (c1 * (HAvg - cAvg * VnAvg));
 
-#if defined(CFD_FAST)
-    double cc = (deltaP + rhoAvg * cAvg * deltaVn) * (0.5 * ic2);
-#else
     double cc = (deltaP + rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
-#endif
     Fd[0] += lambda[2] * (cc * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] += lambda[2] * (cc * (vAvg[i] + cAvg * n[i]));
     Fd[E] += lambda[2] * (cc * (HAvg + cAvg * VnAvg));
 
-#if defined(CFD_FAST)
-    double c2 = deltaRho - deltaP * ic2;
-#else
     double c2 = deltaRho - deltaP / (cAvg * cAvg);
-#endif
     Fd[0] += lambda[1] * (c2 * 1.0 + rhoAvg * 0.0);
     // tangential components carry rhoAvg * dv_i, the normal one 0
     // (fluxSchemes.hpp:526-528 for axis normals).
@@ -1052,6 +1099,7 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     }
     Fd[E] += lambda[1] * (c2 * q_2Avg + rhoAvg * tE);
     for (int i = 0; i < NV; i++) res[i] = (FcL[i] + FcR[i] - Fd[i]) / 2;
+#endif
 }
 
 template <int NV, int AX, int FLUX>
