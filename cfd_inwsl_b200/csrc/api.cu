@@ -491,8 +491,8 @@ int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, doub
 int default_seg_len(const cfd_handle *h, int d)
 {
     int n = h->cfg.n[d];
-    int S = (h->dim == 1) ? 128 : (d == 0 ? 64 : 8);
-    int W = (h->dim == 1) ? 1 : (d == 0 ? 4 : 32);
+    int S = (h->dim == 1) ? cfd::k1S : (d == 0 ? cfd::kXS : cfd::kYS);
+    int W = (h->dim == 1) ? cfd::k1W : (d == 0 ? cfd::kXW : cfd::kYW);
     int t0, t1;
     transverse_axes(d, t0, t1);
     long long blocks_per_seg = (long long)((h->cfg.n[t0] + W - 1) / W) * h->cfg.n[t1];

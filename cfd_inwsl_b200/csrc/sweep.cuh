@@ -23,6 +23,8 @@
 // of a line; along y/z consecutive threads take neighbouring lines (adjacent
 // x), so every global access is coalesced along x in all three sweeps.
 #pragma once
+#include <cuda_pipeline.h>
+
 #include "euler_math.cuh"
 #include "mixed.cuh"
 #include "sweep_params.h"
@@ -105,7 +107,14 @@ struct SweepShape {
     static constexpr int SMEM_DOUBLES = 2 * NV * W * LSP + NV * W * LSF;
     // mixed form: FP32 hi/lo split of the cons ring (exact FP32 increments)
     static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
-    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
+    static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
+    // Asynchronous staging (cp.async) of each thread's global operands: the next
+    // chunk's cell and the epilogue's rhs / U^0 / U^k, so that their latency
+    // hides behind the face phase. Only where two CTAs per SM still fit in the
+    // 228 KB of an SM (1 KB of it reserved per CTA).
+    static constexpr size_t SMEM_STAGE = sizeof(double) * 4 * NV * NT;
+    static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= 112 * 1024;
+    static constexpr size_t SMEM_BYTES = SMEM_RINGS + (PF ? SMEM_STAGE : 0);
 };
 
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
@@ -130,6 +139,9 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     double *sf = sc + NV * W * LSP;      // [NV][W][LSF] face flux
     float *shi = reinterpret_cast<float *>(sf + NV * W * LSF);  // mixed form: [NV][W][LSP] (float)cons
     float *slo = shi + NV * W * LSP;                            //             [NV][W][LSP] cons - hi
+    // staging: [0] next chunk's cons, [1] rhs, [2] U^0, [3] U^k; [NV][NT] each
+    double *stg = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + SH::SMEM_RINGS);
+    constexpr bool PF = SH::PF;
 
     constexpr int T0 = (AX == 0) ? 1 : 0;  // transverse axis with neighbouring lines in a CTA
     constexpr int T1 = (AX == 2) ? 1 : 2;
@@ -157,8 +169,9 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         lid = a + nt0 * bb;
     };
 
-    // Stage cell P (global index along AX, may be a ghost) of line l.
-    auto load_pos = [&](int l, int P) {
+    // Stage cell P (global index along AX, may be a ghost) of line l; staged:
+    // its cons already sit in stg[0] (interior cells of the thread's own line).
+    auto load_pos = [&](int l, int P, bool staged = false) {
         bool ok; long long base; int lid;
         line_of(l, ok, base, lid);
         double pr[NV];
@@ -167,7 +180,14 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             for (int v = 1; v < NV - 1; v++) pr[v] = 0.0;
             pr[NV - 1] = 1.0;
         } else if (P >= 0 && P < nd) {
-            load_cons_prim<NV>(p.u, p.ncell, base + (long long)P * sAX, pr);
+            if (staged) {
+                double c[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) c[v] = stg[v * NT + threadIdx.x];
+                cons_to_prim<NV>(c, pr);
+            } else {
+                load_cons_prim<NV>(p.u, p.ncell, base + (long long)P * sAX, pr);
+            }
         } else if (P < 0) {
             int k = -P - 1;
             ghost_prim<NV>(p, p.bc_lo[lid], k > 3 ? 3 : k, tstage, pr);
@@ -241,8 +261,45 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     double red_rho = 0.0, red_lam[3] = {0.0, 0.0, 0.0};
     unsigned err = 0;
 
+    // cp.async of this thread's interior cell at position P into stg[0]
+    auto prefetch_cell = [&](int P) {
+        bool ok; long long base; int lid;
+        line_of(tl, ok, base, lid);
+        if (ok && P >= 0 && P < nd) {
+            const long long cell = base + (long long)P * sAX;
+#pragma unroll
+            for (int v = 0; v < NV; v++) __pipeline_memcpy_async(stg + v * NT + tid, p.u + v * p.ncell + cell, 8);
+        }
+        __pipeline_commit();
+    };
+    // cp.async of the epilogue operands of this thread's cell i
+    const bool need_rhs = !p.first, need_u0 = p.mode == MODE_RK, need_u = p.mode == MODE_RK && p.rk_stage != 1;
+    auto prefetch_epilogue = [&](int i) {
+        bool ok; long long base; int lid;
+        line_of(tl, ok, base, lid);
+        if (ok && i < s_end) {
+            const long long cell = base + (long long)i * sAX;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const long long gi = v * p.ncell + cell;
+                if (need_rhs) __pipeline_memcpy_async(stg + (1 * NV + v) * NT + tid, p.rhs + gi, 8);
+                if (need_u0) __pipeline_memcpy_async(stg + (2 * NV + v) * NT + tid, p.u0 + gi, 8);
+                if (need_u) __pipeline_memcpy_async(stg + (3 * NV + v) * NT + tid, p.u + gi, 8);
+            }
+        }
+        __pipeline_commit();
+    };
+    if constexpr (PF) prefetch_cell(s_begin + 4 + tp);
+
     for (int c0 = s_begin; c0 < s_end; c0 += S) {
-        load_pos(tl, c0 + 4 + tp);
+        if constexpr (PF) {
+            __pipeline_wait_prior(0);
+            load_pos(tl, c0 + 4 + tp, true);
+            prefetch_epilogue(c0 + tp);
+            prefetch_cell(c0 + S + 4 + tp);  // an empty group past the segment
+        } else {
+            load_pos(tl, c0 + 4 + tp);
+        }
         __syncthreads();
         if (c0 == s_begin) {
             for (int idx = tid; idx < 3 * W; idx += NT) {
@@ -257,6 +314,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         const int i = c0 + tp;
         bool ok; long long base; int lid;
         line_of(tl, ok, base, lid);
+        if constexpr (PF) __pipeline_wait_prior(1);  // the epilogue operands; the next cell may still fly
         if (ok && i < s_end) {
             double pm[NV], pp[NV], fnm[NV], fnp[NV];
             int sm = ring(i - 1 - s_begin + 4), spp = ring(i + 1 - s_begin + 4);
@@ -276,7 +334,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 const double *fv = sf + (v * W + tl) * LSF;
                 double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
-                double r = p.first ? (0.0 + d) : (p.rhs[gi] + d);
+                const double *sv = stg + v * NT + tid;
+                double r = p.first ? (0.0 + d) : ((PF ? sv[1 * NV * NT] : p.rhs[gi]) + d);
                 if constexpr (NV == 4) {
                     // SourceTerm::calGravitySource (sourceTerm.cpp:3-20) on the
                     // stage's prim: rhs(rho v) -= rho, rhs(rho E) -= rho v
@@ -292,10 +351,11 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 } else {
                     if (v == 0 && p.want_reduce) red_rho = fmax(red_rho, fabs(r));
                     double o;
+                    const double u0v = PF ? sv[2 * NV * NT] : p.u0[gi];
                     if (p.rk_stage == 1) {
-                        o = p.u0[gi] - rkBdt * r;
+                        o = u0v - rkBdt * r;
                     } else {
-                        o = p.rkA * p.u0[gi] - rkBdt * r + p.rkC * p.u[gi];
+                        o = p.rkA * u0v - rkBdt * r + p.rkC * (PF ? sv[3 * NV * NT] : p.u[gi]);
                     }
                     uo[v] = o;
                     p.u_out[gi] = o;
@@ -451,26 +511,26 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
     return cudaErrorInvalidValue;
 }
 
-// Tile shapes: along x, 64 cells x 4 lines; along y/z, 8 cells x 32 lines
-// (1D: 128 cells of one line).
+// Tile shapes (kXS x kXW along x, kYS x kYW along y/z, k1S x k1W in 1D): see
+// sweep_params.h.
 template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st)
 {
     if constexpr (NV == 3) {
         if (ax != 0) return cudaErrorInvalidValue;
-        return flux == FLUX_HLLC ? launch_sweep_shape<3, 0, FAM, FLUX_HLLC, 128, 1>(p, st)
-                                 : launch_sweep_shape<3, 0, FAM, FLUX_ROE, 128, 1>(p, st);
+        return flux == FLUX_HLLC ? launch_sweep_shape<3, 0, FAM, FLUX_HLLC, k1S, k1W>(p, st)
+                                 : launch_sweep_shape<3, 0, FAM, FLUX_ROE, k1S, k1W>(p, st);
     } else {
         if (ax == 0)
-            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, 64, 4>(p, st)
-                                     : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, 64, 4>(p, st);
+            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, kXS, kXW>(p, st)
+                                     : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, kXS, kXW>(p, st);
         if (ax == 1)
-            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 1, FAM, FLUX_HLLC, 8, 32>(p, st)
-                                     : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, 8, 32>(p, st);
+            return flux == FLUX_HLLC ? launch_sweep_shape<NV, 1, FAM, FLUX_HLLC, kYS, kYW>(p, st)
+                                     : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, kYS, kYW>(p, st);
         if constexpr (NV == 5) {
             if (ax == 2)
-                return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, 8, 32>(p, st)
-                                         : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, 8, 32>(p, st);
+                return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, kYS, kYW>(p, st)
+                                         : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, kYS, kYW>(p, st);
         }
         return cudaErrorInvalidValue;
     }
@@ -482,19 +542,19 @@ cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStre
 {
     if constexpr (NV == 3) {
         if (ax != 0) return cudaErrorInvalidValue;
-        return flux == FLUX_HLLC ? launch_batched_shape<3, 0, FAM, FLUX_HLLC, 128, 1>(b, st)
-                                 : launch_batched_shape<3, 0, FAM, FLUX_ROE, 128, 1>(b, st);
+        return flux == FLUX_HLLC ? launch_batched_shape<3, 0, FAM, FLUX_HLLC, k1S, k1W>(b, st)
+                                 : launch_batched_shape<3, 0, FAM, FLUX_ROE, k1S, k1W>(b, st);
     } else {
         if (ax == 0)
-            return flux == FLUX_HLLC ? launch_batched_shape<NV, 0, FAM, FLUX_HLLC, 64, 4>(b, st)
-                                     : launch_batched_shape<NV, 0, FAM, FLUX_ROE, 64, 4>(b, st);
+            return flux == FLUX_HLLC ? launch_batched_shape<NV, 0, FAM, FLUX_HLLC, kXS, kXW>(b, st)
+                                     : launch_batched_shape<NV, 0, FAM, FLUX_ROE, kXS, kXW>(b, st);
         if (ax == 1)
-            return flux == FLUX_HLLC ? launch_batched_shape<NV, 1, FAM, FLUX_HLLC, 8, 32>(b, st)
-                                     : launch_batched_shape<NV, 1, FAM, FLUX_ROE, 8, 32>(b, st);
+            return flux == FLUX_HLLC ? launch_batched_shape<NV, 1, FAM, FLUX_HLLC, kYS, kYW>(b, st)
+                                     : launch_batched_shape<NV, 1, FAM, FLUX_ROE, kYS, kYW>(b, st);
         if constexpr (NV == 5) {
             if (ax == 2)
-                return flux == FLUX_HLLC ? launch_batched_shape<NV, 2, FAM, FLUX_HLLC, 8, 32>(b, st)
-                                         : launch_batched_shape<NV, 2, FAM, FLUX_ROE, 8, 32>(b, st);
+                return flux == FLUX_HLLC ? launch_batched_shape<NV, 2, FAM, FLUX_HLLC, kYS, kYW>(b, st)
+                                         : launch_batched_shape<NV, 2, FAM, FLUX_ROE, kYS, kYW>(b, st);
         }
         return cudaErrorInvalidValue;
     }

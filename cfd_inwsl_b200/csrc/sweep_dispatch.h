@@ -55,7 +55,7 @@ inline long long sweep_tile_count(int nv, int ax, const SweepParams &p)
 {
     int T0 = (nv == 3) ? 1 : ((ax == 0) ? 1 : 0);
     int T1 = (ax == 2) ? 1 : 2;
-    int W = (nv == 3) ? 1 : ((ax == 0) ? 4 : 32);
+    int W = (nv == 3) ? k1W : ((ax == 0) ? kXW : kYW);
     long long nseg = (p.n[ax] + p.seg_len - 1) / p.seg_len;
     return (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
 }

@@ -4,6 +4,18 @@
 
 namespace cfd {
 
+// Tile shapes of the sweeps: cells per chunk (S) x lines per CTA (W).
+#ifndef CFD_XS
+#define CFD_XS 64
+#endif
+#ifndef CFD_XW
+#define CFD_XW 4
+#endif
+constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
+constexpr int kYS = 8, kYW = 32;           // along y and z
+constexpr int k1S = 128, k1W = 1;          // 1D
+
+
 // BndType values (zone_FD/src/include/macro.hpp:33-34) plus the 3D mirror.
 enum : int {
     BND_TYPENULL = 0,
