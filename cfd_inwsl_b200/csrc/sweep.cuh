@@ -112,8 +112,12 @@ struct SweepShape {
     // chunk's cell and the epilogue's rhs / U^0 / U^k, so that their latency
     // hides behind the face phase. Only where two CTAs per SM still fit in the
     // 228 KB of an SM (1 KB of it reserved per CTA).
-    static constexpr size_t SMEM_STAGE = sizeof(double) * 4 * NV * NT;
+    // The x sweep of a 2D/3D step is always the first direction (no epilogue
+    // operands to stage), so it stages only the next chunk's cells.
+    static constexpr int NSTG = (AX == 0 && NV >= 4) ? 1 : 4;
+    static constexpr size_t SMEM_STAGE = sizeof(double) * NSTG * NV * NT;
     static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= 112 * 1024;
+    static constexpr bool PF_EPI = PF && NSTG == 4;
     static constexpr size_t SMEM_BYTES = SMEM_RINGS + (PF ? SMEM_STAGE : 0);
 };
 
@@ -141,7 +145,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     float *slo = shi + NV * W * LSP;                            //             [NV][W][LSP] cons - hi
     // staging: [0] next chunk's cons, [1] rhs, [2] U^0, [3] U^k; [NV][NT] each
     double *stg = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + SH::SMEM_RINGS);
-    constexpr bool PF = SH::PF;
+    constexpr bool PF = SH::PF, PF_EPI = SH::PF_EPI;
 
     constexpr int T0 = (AX == 0) ? 1 : 0;  // transverse axis with neighbouring lines in a CTA
     constexpr int T1 = (AX == 2) ? 1 : 2;
@@ -273,7 +277,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         __pipeline_commit();
     };
     // cp.async of the epilogue operands of this thread's cell i
-    const bool need_rhs = !p.first, need_u0 = p.mode == MODE_RK, need_u = p.mode == MODE_RK && p.rk_stage != 1;
+    const bool need_rhs = PF_EPI && !p.first, need_u0 = PF_EPI && p.mode == MODE_RK,
+               need_u = PF_EPI && p.mode == MODE_RK && p.rk_stage != 1;
     auto prefetch_epilogue = [&](int i) {
         bool ok; long long base; int lid;
         line_of(tl, ok, base, lid);
@@ -335,7 +340,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
                 const double *sv = stg + v * NT + tid;
-                double r = p.first ? (0.0 + d) : ((PF ? sv[1 * NV * NT] : p.rhs[gi]) + d);
+                double r = p.first ? (0.0 + d) : ((PF_EPI ? sv[1 * NV * NT] : p.rhs[gi]) + d);
                 if constexpr (NV == 4) {
                     // SourceTerm::calGravitySource (sourceTerm.cpp:3-20) on the
                     // stage's prim: rhs(rho v) -= rho, rhs(rho E) -= rho v
@@ -351,11 +356,11 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 } else {
                     if (v == 0 && p.want_reduce) red_rho = fmax(red_rho, fabs(r));
                     double o;
-                    const double u0v = PF ? sv[2 * NV * NT] : p.u0[gi];
+                    const double u0v = PF_EPI ? sv[2 * NV * NT] : p.u0[gi];
                     if (p.rk_stage == 1) {
                         o = u0v - rkBdt * r;
                     } else {
-                        o = p.rkA * u0v - rkBdt * r + p.rkC * (PF ? sv[3 * NV * NT] : p.u[gi]);
+                        o = p.rkA * u0v - rkBdt * r + p.rkC * (PF_EPI ? sv[3 * NV * NT] : p.u[gi]);
                     }
                     uo[v] = o;
                     p.u_out[gi] = o;
