@@ -89,6 +89,9 @@ _PROTOS = {
     "cfd_launch_count": (C.c_ulonglong, [C.c_void_p]),
     "cfd_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double]),
     "cfd_rhs_noalloc": (C.c_int, [C.POINTER(CfdConfig), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    "cfd_rhs_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cfd_adjoint_record": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
+    "cfd_adjoint_reverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 

@@ -12,7 +12,9 @@
 #include "euler_math.cuh"
 #include "mixed.cuh"
 #include "sweep_dispatch.h"
+#include "adjoint.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -264,6 +266,12 @@ struct cfd_handle {
     // captured step graphs, by (steps per graph index: 1, 3, 12) x (start slot)
     cudaGraphExec_t graph[3][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     unsigned long long launches = 0;     // kernels this library launched
+    // discrete adjoint: forward checkpoints and reverse work buffers
+    std::vector<double *> adj_ckpt;      // state at steps 0, K, 2K, ... of the recorded run
+    std::vector<double *> adj_stage;     // U^0, U^(1), U^(2) of each step of one segment
+    double *adj_buf[4] = {nullptr, nullptr, nullptr, nullptr};  // lambda, w, w2, face scratch (24 states)
+    double adj_dt = 0.0;
+    int adj_nsteps = 0, adj_every = 0;
 };
 
 namespace {
@@ -707,6 +715,9 @@ void cfd_destroy(cfd_handle *h)
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
     cudaFree(h->d_dts);
     cudaFree(h->d_linf);
+    for (double *b : h->adj_ckpt) cudaFree(b);
+    for (double *b : h->adj_stage) cudaFree(b);
+    for (double *b : h->adj_buf) cudaFree(b);
     drop_graphs(h);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -1406,3 +1417,174 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ discrete adjoint
+
+namespace {
+
+int adjoint_supported(cfd_handle *h)
+{
+    if (h->dim != 2 || h->fam != cfd::FAM_WCNS5 || h->cfg.flux_method != CFD_FLUX_ROE ||
+        h->cfg.precision != CFD_PREC_FP64 || h->cfg.source_type != 0)
+        return fail(h, CFD_ERR_UNSUPPORTED, "the adjoint covers 2D WCNS5 + Roe, FP64, without source terms");
+    for (int d = 0; d < 2; d++)
+        for (int sd = 0; sd < 2; sd++)
+            if (h->cfg.bc[d][sd] != CFD_BND_PERIODIC_WRAP)
+                return fail(h, CFD_ERR_UNSUPPORTED, "the adjoint needs periodic (CFD_BND_PERIODIC_WRAP) boundaries");
+    return CFD_OK;
+}
+
+int adjoint_buffers(cfd_handle *h)
+{
+    const size_t state = sizeof(double) * h->ncell * h->nv;
+    for (int k = 0; k < 4; k++) {
+        if (h->adj_buf[k]) continue;
+        cudaError_t e = cudaMalloc(&h->adj_buf[k], k == 3 ? 6 * state : state);
+        if (e != cudaSuccess) {
+            h->adj_buf[k] = nullptr;
+            return fail(h, CFD_ERR_NOMEM, "adjoint work buffers");
+        }
+    }
+    return CFD_OK;
+}
+
+// w = (dR/dU)^T mu at the state U (both directions)
+int rhs_vjp(cfd_handle *h, const double *U, const double *mu, double *w)
+{
+    const int nx = h->cfg.n[0], ny = h->cfg.n[1];
+    for (int d = 0; d < 2; d++) {
+        cudaError_t e =
+            cfd::adj::launch_sweep_vjp(d, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[d], d > 0, h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
+        h->launches += 2;
+    }
+    return CFD_OK;
+}
+
+int axpby(cfd_handle *h, double a, const double *x, double b, double *y)
+{
+    cudaError_t e = cfd::adj::launch_axpby(a, x, b, y, h->ncell * h->nv, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint axpby");
+    h->launches += 1;
+    return CFD_OK;
+}
+
+void adjoint_release(std::vector<double *> &v)
+{
+    for (double *b : v) cudaFree(b);
+    v.clear();
+}
+
+int adjoint_states(cfd_handle *h, std::vector<double *> &v, size_t count)
+{
+    const size_t state = sizeof(double) * h->ncell * h->nv;
+    while (v.size() < count) {
+        double *b = nullptr;
+        if (cudaMalloc(&b, state) != cudaSuccess) return fail(h, CFD_ERR_NOMEM, "adjoint checkpoints");
+        v.push_back(b);
+    }
+    return CFD_OK;
+}
+
+// one SSP-RK3 step with frozen dt from S[0], keeping its stage states in S[1], S[2]; out = U^(n+1)
+int adjoint_step(cfd_handle *h, double dt, double *const *S, double *out)
+{
+    int rc;
+    if ((rc = rk_stage(h, 1, S[0], S[0], S[1], 1.0, dt, 0.0, 0.0, false))) return rc;
+    if ((rc = rk_stage(h, 2, S[1], S[0], S[2], 0.75, 0.25 * dt, 0.25, 0.0, false))) return rc;
+    return rk_stage(h, 3, S[2], S[0], out, 1.0 / 3.0, 2.0 / 3.0 * dt, 2.0 / 3.0, 0.0, false);
+}
+
+} // namespace
+
+int cfd_rhs_vjp(cfd_handle *h, const double *mu_aos, double *lam_aos)
+{
+    if (!h || !mu_aos || !lam_aos) return CFD_ERR_CONFIG;
+    int rc;
+    if ((rc = adjoint_supported(h)) || (rc = adjoint_buffers(h))) return rc;
+    CFD_CUDA(h, cudaMemcpyAsync(h->stage, mu_aos, sizeof(double) * h->ncell * h->nv, cudaMemcpyHostToDevice,
+                                h->stream));
+    if ((rc = launch_aos_to_soa(h, h->stage, h->adj_buf[0]))) return rc;
+    if ((rc = rhs_vjp(h, h->u[h->cur], h->adj_buf[0], h->adj_buf[1]))) return rc;
+    if ((rc = launch_soa_to_aos(h, h->adj_buf[1], h->stage, 0))) return rc;
+    CFD_CUDA(h, cudaMemcpyAsync(lam_aos, h->stage, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToHost,
+                                h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}
+
+int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
+{
+    if (!h || nsteps < 1 || ckpt_every < 1 || !(dt > 0.0)) return CFD_ERR_CONFIG;
+    int rc;
+    if ((rc = adjoint_supported(h)) || (rc = sync_bc(h))) return rc;
+    const size_t nck = (size_t)((nsteps + ckpt_every - 1) / ckpt_every);
+    adjoint_release(h->adj_ckpt);
+    if ((rc = adjoint_states(h, h->adj_ckpt, nck))) return rc;
+    const size_t state = sizeof(double) * h->ncell * h->nv;
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+    for (int s = 0; s < nsteps; s++) {
+        double *U0 = h->u[h->cur], *U1 = h->u[(h->cur + 1) % 3], *U2 = h->u[(h->cur + 2) % 3];
+        if (s % ckpt_every == 0)
+            CFD_CUDA(h, cudaMemcpyAsync(h->adj_ckpt[s / ckpt_every], U0, state, cudaMemcpyDeviceToDevice, h->stream));
+        double *S[3] = {U0, U1, U2};
+        if ((rc = adjoint_step(h, dt, S, U1))) return rc;
+        h->cur = (h->cur + 1) % 3;
+    }
+    h->ws_valid = false;
+    h->adj_dt = dt;
+    h->adj_nsteps = nsteps;
+    h->adj_every = ckpt_every;
+    unsigned err = 0;
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return check_err(h, err);
+}
+
+int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_aos)
+{
+    if (!h || !dJ_dUN_aos || !dJ_dU0_aos) return CFD_ERR_CONFIG;
+    if (h->adj_nsteps < 1) return fail(h, CFD_ERR_CONFIG, "cfd_adjoint_reverse needs a cfd_adjoint_record run first");
+    int rc;
+    if ((rc = adjoint_supported(h)) || (rc = adjoint_buffers(h))) return rc;
+    const int K = h->adj_every, N = h->adj_nsteps;
+    const double dt = h->adj_dt;
+    if ((rc = adjoint_states(h, h->adj_stage, 3 * (size_t)K + 1))) return rc;
+    const size_t state = sizeof(double) * h->ncell * h->nv;
+    double *lam = h->adj_buf[0], *w = h->adj_buf[1], *w2 = h->adj_buf[2];
+    CFD_CUDA(h, cudaMemcpyAsync(h->stage, dJ_dUN_aos, state, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = launch_aos_to_soa(h, h->stage, lam))) return rc;
+    const int nseg = (N + K - 1) / K;
+    for (int seg = nseg - 1; seg >= 0; seg--) {
+        const int s0 = seg * K, cnt = std::min(K, N - s0);
+        // recompute the segment, keeping every stage state
+        CFD_CUDA(h, cudaMemcpyAsync(h->adj_stage[0], h->adj_ckpt[seg], state, cudaMemcpyDeviceToDevice, h->stream));
+        for (int j = 0; j < cnt; j++) {
+            double *S[3] = {h->adj_stage[3 * j], h->adj_stage[3 * j + 1], h->adj_stage[3 * j + 2]};
+            if (j + 1 < cnt && (rc = adjoint_step(h, dt, S, h->adj_stage[3 * (j + 1)]))) return rc;
+            if (j + 1 == cnt) {
+                // the last step's stages only (its output is not needed)
+                if ((rc = rk_stage(h, 1, S[0], S[0], S[1], 1.0, dt, 0.0, 0.0, false))) return rc;
+                if ((rc = rk_stage(h, 2, S[1], S[0], S[2], 0.75, 0.25 * dt, 0.25, 0.0, false))) return rc;
+            }
+        }
+        // reverse through the segment's steps:
+        //   U1 = U0 - dt R(U0); U2 = 3/4 U0 + 1/4 (U1 - dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 - dt R(U2))
+        for (int j = cnt - 1; j >= 0; j--) {
+            double *U0 = h->adj_stage[3 * j], *U1 = h->adj_stage[3 * j + 1], *U2 = h->adj_stage[3 * j + 2];
+            if ((rc = rhs_vjp(h, U2, lam, w))) return rc;                 // w = J(U2)^T lam3
+            if ((rc = axpby(h, 2.0 / 3.0, lam, -2.0 / 3.0 * dt, w))) return rc;  // w = lam2
+            if ((rc = axpby(h, 0.0, lam, 1.0 / 3.0, lam))) return rc;     // lam = lam3 / 3
+            if ((rc = rhs_vjp(h, U1, w, w2))) return rc;                  // w2 = J(U1)^T lam2
+            if ((rc = axpby(h, 0.25, w, -0.25 * dt, w2))) return rc;      // w2 = lam1
+            if ((rc = axpby(h, 0.75, w, 1.0, lam))) return rc;            // lam += 3/4 lam2
+            if ((rc = rhs_vjp(h, U0, w2, w))) return rc;                  // w = J(U0)^T lam1
+            if ((rc = axpby(h, 1.0, w2, 1.0, lam))) return rc;            // lam += lam1
+            if ((rc = axpby(h, -dt, w, 1.0, lam))) return rc;             // lam -= dt w
+        }
+    }
+    if ((rc = launch_soa_to_aos(h, lam, h->stage, 0))) return rc;
+    CFD_CUDA(h, cudaMemcpyAsync(dJ_dU0_aos, h->stage, state, cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}

@@ -356,6 +356,25 @@ class BlockSolver:
                 linfs.append(linf)
         return (np.array(dts), np.array(linfs)) if record else None
 
+    # --- discrete adjoint (no counterpart in the reference)
+    def rhs_vjp(self, mu: np.ndarray) -> np.ndarray:
+        """(dR/dU)^T mu at the current state (cfd_rhs_vjp); mu, result: AoS (ncell, nvar)."""
+        m = np.ascontiguousarray(mu, dtype=np.float64).reshape(self.ncell, self.nvar)
+        out = np.empty_like(m)
+        _lib.check(self.lib.cfd_rhs_vjp(self.h, _lib.ptr(m), _lib.ptr(out)), self.h)
+        return out
+
+    def adjoint_record(self, dt: float, nsteps: int, ckpt_every: int = 20):
+        """Forward run of nsteps frozen-dt RK3 steps with checkpoints (cfd_adjoint_record)."""
+        _lib.check(self.lib.cfd_adjoint_record(self.h, float(dt), int(nsteps), int(ckpt_every)), self.h)
+
+    def adjoint_reverse(self, dJ_dUN: np.ndarray) -> np.ndarray:
+        """dJ/dU^0 from dJ/dU^N of the recorded run (cfd_adjoint_reverse)."""
+        g = np.ascontiguousarray(dJ_dUN, dtype=np.float64).reshape(self.ncell, self.nvar)
+        out = np.empty_like(g)
+        _lib.check(self.lib.cfd_adjoint_reverse(self.h, _lib.ptr(g), _lib.ptr(out)), self.h)
+        return out
+
     def run_device(self, max_steps: int = 1 << 30):
         """Device-resident stepsLoopCFL (cfd_run): returns (dts, linfs)."""
         info = self.info

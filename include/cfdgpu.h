@@ -228,6 +228,31 @@ unsigned long long cfd_batch_launch_count(const cfd_batch *b);
 int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_dt, int max_steps, double *t,
                   int *nsteps);
 
+/* Discrete adjoint. The reference has no adjoint; these entry points serve
+ * gradient studies of the same discretisation (sensitivity of a functional of
+ * the final state to the initial state). They cover 2D handles with WCNS5
+ * (weno5_JSchen) reconstruction, the Roe flux, FP64, no source term and
+ * CFD_BND_PERIODIC_WRAP on every side (CFD_ERR_UNSUPPORTED otherwise); the
+ * positivity fallback is differentiated where it fires.
+ *
+ * cfd_rhs_vjp: lam = (dR/dU)^T mu at the handle's current state, R the RHS of
+ * cfd_rhs (SpDistributor::rhsSolve, sp_distributor.cpp:3-79); mu and lam are
+ * host AoS arrays like the state.
+ *
+ * cfd_adjoint_record: from the current state U^0, runs nsteps SSP-RK3 steps
+ * with the fixed step dt (BlockSolver::RK3_SSP, blockSolver.cpp:43-87, dt
+ * frozen so that the map U^0 -> U^N is differentiable) and keeps the state of
+ * every ckpt_every-th step on the device. The handle's state is U^N afterwards.
+ *
+ * cfd_adjoint_reverse: given dJ/dU^N (host AoS), returns dJ/dU^0 (host AoS):
+ * segment by segment backwards, it recomputes the segment's steps from its
+ * checkpoint (keeping the three stage states of each step) and applies the
+ * transposed stage Jacobians. Device memory: nsteps / ckpt_every + 3 *
+ * ckpt_every + 9 states. */
+int cfd_rhs_vjp(cfd_handle *h, const double *mu, double *lam);
+int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every);
+int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN, double *dJ_dU0);
+
 /* Library version string. */
 const char *cfd_version(void);
 
