@@ -211,6 +211,73 @@ def vortex_accuracy(n, L, im, fm, cfl, device, t_end=2.0):
     return out
 
 
+def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
+    """Adjoint configuration: 256^2 periodic [0,1]^2, rho = 1 + drho (seeded
+    Gaussian-filtered noise, correlation length 0.05, RMS 1e-2), p = 1/gamma,
+    (u, v) = (0.5, 0.3), WCNS5 + Roe, 400 frozen-dt RK3 steps (dt from CFL 0.5 at
+    t = 0), checkpoints every 20 steps, J = sum of rho^2 over 64 seeded probe
+    cells. Times, with CUDA events on the handle's stream: the forward steps,
+    cfd_adjoint_record (forward with checkpoints) and cfd_adjoint_reverse
+    (segment recomputation + transposed stage Jacobians)."""
+    import torch
+    from cfd_inwsl_b200 import _lib, zone
+    rng = np.random.default_rng(seed)
+    k = np.fft.fftfreq(n, d=1.0 / n)
+    KX, KY = np.meshgrid(k, k)
+    noise = rng.normal(size=(n, n))
+    filt = np.exp(-0.5 * (2 * np.pi * 0.05) ** 2 * (KX ** 2 + KY ** 2))
+    drho = np.real(np.fft.ifft2(np.fft.fft2(noise) * filt))
+    drho *= 1e-2 / np.sqrt(np.mean(drho ** 2))
+    rho = 1.0 + drho.reshape(-1)
+    gamma = 1.4
+    cons = np.stack([rho, 0.5 * rho, 0.3 * rho, (1 / gamma) / (gamma - 1) + 0.5 * rho * (0.25 + 0.09)], -1)
+    info = zone.Info()
+    info.dim = 2
+    info.iMax = [n + 1, n + 1, 1]
+    info.calZone = [0, 1, 0, 1, 0, 0]
+    info.interMethod = 2
+    info.fluxMethod = 1
+    info.CFL = 0.5
+    info.device = device
+    s = zone.BlockSolver(info, periodic=True)
+    _lib.check(s.lib.cfd_set_stream(s.h, C.c_void_p(stream.cuda_stream)), s.h)
+    s.set_cons(cons)
+    dt = s.getTimeIntervalExplicit()
+    probes = rng.choice(n * n, 64, replace=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def forward():
+        for _ in range(nsteps):
+            _lib.check(s.lib.cfd_rk3_step(s.h, dt, 0.0, None), s.h)
+
+    s.set_cons(cons)
+    forward()  # warm-up
+    s.set_cons(cons)
+    fwd_ms = timed(forward)
+    s.set_cons(cons)
+    rec_ms = timed(lambda: s.adjoint_record(dt, nsteps, ckpt))
+    UN = s.cons
+    seed_g = np.zeros_like(UN)
+    seed_g[probes, 0] = 2 * UN[probes, 0]
+    out = {}
+    rev_ms = timed(lambda: out.setdefault("g", s.adjoint_reverse(seed_g)))
+    J = float(np.sum(UN[probes, 0] ** 2))
+    s.close()
+    return {"config": "256^2 periodic, WCNS5 + Roe, 400 frozen-dt RK3 steps, checkpoints every 20, "
+                      "J = sum of rho^2 over 64 probes",
+            "forward_ms": fwd_ms, "record_ms": rec_ms, "reverse_ms": rev_ms,
+            "reverse_over_forward": rev_ms / fwd_ms, "record_plus_reverse_over_forward": (rec_ms + rev_ms) / fwd_ms,
+            "J": J, "grad_l2": float(np.linalg.norm(out["g"]))}
+
+
 # --------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -361,6 +428,10 @@ def run_ours(args, rank, world, local_rank):
         if dim == 2 and rank == 0:
             mixed["l1_rho_vs_exact"] = vortex_accuracy(args.accuracy_grid, L, im, fm, cfl, local_rank)
 
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        adjoint = adjoint_cost(local_rank, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_throughput(dim, n, L, im, fm, cfl, budget_s=args.cpu_budget)
@@ -389,6 +460,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if mixed is not None:
         result["mixed"] = mixed
+    if adjoint is not None:
+        result["adjoint"] = adjoint
     if cpu is not None:
         result["cpu_baseline"] = cpu
     solver.close()
@@ -405,6 +478,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="form of the timed steps (mixed: CFD_PREC_MIXED)")
     ap.add_argument("--accuracy-grid", type=int, default=512)
