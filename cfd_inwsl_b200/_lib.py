@@ -92,6 +92,10 @@ _PROTOS = {
     "cfd_rhs_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "cfd_adjoint_record": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
     "cfd_adjoint_reverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cfd_enable_halo": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
+    "cfd_stage_state": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cfd_rk3_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
+    "cfd_max_wave_speeds": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 

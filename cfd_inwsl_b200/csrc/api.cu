@@ -272,6 +272,8 @@ struct cfd_handle {
     double *adj_buf[4] = {nullptr, nullptr, nullptr, nullptr};  // lambda, w, w2, face scratch (24 states)
     double adj_dt = 0.0;
     int adj_nsteps = 0, adj_every = 0;
+    // slab decomposition: halo rows of the last direction's low / high side
+    double *halo[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -441,6 +443,9 @@ SweepParams base_params(cfd_handle *h, int d)
     p.prec = h->cfg.precision == CFD_PREC_MIXED ? 1 : 0;
     p.dm_u = h->dm_u;
     p.dm_v = h->dm_v;
+    p.halo_lo = h->halo[0];
+    p.halo_hi = h->halo[1];
+    p.halo_nl = h->ncell / h->cfg.n[h->dim - 1];
     return p;
 }
 
@@ -718,6 +723,8 @@ void cfd_destroy(cfd_handle *h)
     for (double *b : h->adj_ckpt) cudaFree(b);
     for (double *b : h->adj_stage) cudaFree(b);
     for (double *b : h->adj_buf) cudaFree(b);
+    cudaFree(h->halo[0]);
+    cudaFree(h->halo[1]);
     drop_graphs(h);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -1586,5 +1593,81 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
     if ((rc = launch_soa_to_aos(h, lam, h->stage, 0))) return rc;
     CFD_CUDA(h, cudaMemcpyAsync(dJ_dU0_aos, h->stage, state, cudaMemcpyDeviceToHost, h->stream));
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CFD_OK;
+}
+
+// ------------------------------------------------------------------ slab decomposition
+
+int cfd_enable_halo(cfd_handle *h, int side, double **buf, long long *count)
+{
+    if (!h || !buf || !count || (side != 0 && side != 1) || h->dim < 2) return CFD_ERR_CONFIG;
+    const int d = h->dim - 1;
+    const long long nl = nlines(h, d);
+    const long long n = (long long)h->nv * 4 * nl;
+    if (!h->halo[side]) {
+        CFD_CUDA(h, cudaMalloc(&h->halo[side], sizeof(double) * n));
+        CFD_CUDA(h, cudaMemsetAsync(h->halo[side], 0, sizeof(double) * n, h->stream));
+    }
+    for (long long lid = 0; lid < nl; lid++) {
+        BcLine b;
+        std::memset(&b, 0, sizeof(b));
+        b.type = cfd::BND_HALO;
+        b.i0 = lid;
+        b.offset = side;
+        b.slot = -1;
+        (side == 0 ? h->bc_lo[d] : h->bc_hi[d])[lid] = b;
+    }
+    h->bc_dirty = true;
+    drop_graphs(h);
+    *buf = h->halo[side];
+    *count = n;
+    return CFD_OK;
+}
+
+int cfd_stage_state(cfd_handle *h, int stage, double **state)
+{
+    if (!h || !state || stage < 1 || stage > 3) return CFD_ERR_CONFIG;
+    *state = h->u[(h->cur + stage - 1) % 3];
+    return CFD_OK;
+}
+
+int cfd_rk3_stage(cfd_handle *h, int stage, double dt, double t)
+{
+    if (!h || stage < 1 || stage > 3) return CFD_ERR_CONFIG;
+    int rc = sync_bc(h);
+    if (rc) return rc;
+    double *U0 = h->u[h->cur], *U1 = h->u[(h->cur + 1) % 3], *U2 = h->u[(h->cur + 2) % 3];
+    // stage times follow info->t in RK3_SSP: t, t + dt, (t + dt) - dt/2
+    const double t2 = t + dt, t3 = t2 - dt / 2;
+    if (stage == 1) {
+        CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+        return rk_stage(h, 1, U0, U0, U1, 1.0, dt, 0.0, t, false);
+    }
+    if (stage == 2) return rk_stage(h, 2, U1, U0, U2, 0.75, 0.25 * dt, 0.25, t2, false);
+    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
+    if ((rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 2.0 / 3.0 * dt, 2.0 / 3.0, t3, true))) return rc;
+    h->cur = (h->cur + 1) % 3;
+    h->ws_valid = true;
+    unsigned err;
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return check_err(h, err);
+}
+
+int cfd_max_wave_speeds(cfd_handle *h, double *lam)
+{
+    if (!h || !lam) return CFD_ERR_CONFIG;
+    unsigned long long r[4];
+    if (!h->ws_valid) {
+        int rc = launch_wave_speed(h);
+        if (rc) return rc;
+    }
+    CFD_CUDA(h, cudaMemcpyAsync(r, h->red, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; d++) {
+        double l = 0.0;
+        if (d < h->dim) std::memcpy(&l, &r[1 + d], sizeof(double));
+        lam[d] = l;
+    }
     return CFD_OK;
 }

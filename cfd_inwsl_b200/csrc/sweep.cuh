@@ -82,6 +82,17 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
         if (NV == 5) pr[3] = 0.0;
         return;
     }
+    case BND_HALO: {
+        // rows of the neighbouring slab, ascending: the low side's nearest
+        // ghost is the neighbour's last row, the high side's its first
+        const int r = (bl.offset == 0) ? 3 - k : k;
+        const double *hb = (bl.offset == 0) ? p.halo_lo : p.halo_hi;
+        double c[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) c[v] = hb[((long long)v * 4 + r) * p.halo_nl + bl.i0];
+        cons_to_prim<NV>(c, pr);
+        return;
+    }
     default:
         // DIRICLET and every type whose update() is a no-op keep their static data.
         for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * 4 + k) * NV + v] : 0.0;

@@ -27,6 +27,7 @@ enum : int {
     BND_SYMMETRYX = 10,
     BND_SYMMETRYY = 11,
     BND_SYMMETRYZ = 12,
+    BND_HALO = 101,      // ghost cells from a neighbour's rows (slab decomposition): i0 = line, offset = side
 };
 
 // One line end's ghost wiring, the device image of a OneDBnd
@@ -84,6 +85,8 @@ struct SweepParams {
     int seg_len;        // cells per CTA segment along the sweep
     int prec;           // 0: FP64 reconstruction, 1: mixed FP32/FP64 (fast flavour only)
     int gravity;        // 1: add the gravity source of the stage's input state (last direction only)
+    const double *halo_lo, *halo_hi;  // BND_HALO ghosts: [var][4 rows, ascending][line]
+    long long halo_nl;                // lines per halo row
 };
 
 // One batched sweep launch: the parameter blocks of every case (device array)

@@ -67,6 +67,8 @@ extern "C" {
 #define CFD_BND_SYMMETRYZ 12        /* extension for 3D: mirror, w negated */
 #define CFD_BND_PERIODIC_WRAP 100   /* extension: PERIODIC1D wired as a true wrap
                                        (low side copies the far end, high side the near end) */
+#define CFD_BND_HALO 101            /* extension: ghosts from a neighbouring slab's rows
+                                       (cfd_enable_halo; slab decomposition over GPUs) */
 
 typedef struct cfd_config {
     int dim;            /* 1, 2 or 3 */
@@ -252,6 +254,29 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
 int cfd_rhs_vjp(cfd_handle *h, const double *mu, double *lam);
 int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every);
 int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN, double *dJ_dU0);
+
+/* Slab decomposition of one grid over several GPUs (no counterpart in the
+ * reference, which runs one block on one host). Each rank's handle holds a
+ * slab along the last direction (y in 2D, z in 3D) and takes the ghost cells
+ * of that direction's slab interfaces from halo buffers that the caller fills
+ * with the neighbouring slab's four boundary rows (planes) before every stage:
+ *
+ * cfd_enable_halo: wires every line end of `side` (0 low, 1 high) of the last
+ *   direction as CFD_BND_HALO and returns the device halo buffer, planar
+ *   [var][row][line] with 4 rows in ascending coordinate order and
+ *   n[0] (2D) or n[0]*n[1] (3D) lines; *count = nvar * 4 * lines doubles.
+ * cfd_stage_state: device pointer of stage `stage`'s input state (1: U^n,
+ *   2: U^(1), 3: U^(2)), planar SoA; its first and last four rows (planes) of
+ *   the last direction are what the neighbours need.
+ * cfd_rk3_stage: one stage of cfd_rk3_step (stage 3 completes the step and
+ *   makes U^(n+1) the current state); t is the step's start time.
+ * cfd_max_wave_speeds: max over cells of (c + |u_d|) / h_d per direction d
+ *   (the terms of getTimeIntervalExplicit's sum, blockSolver.cpp:318-349), so
+ *   that ranks can take the maximum over slabs before dt = CFL / sum_d. */
+int cfd_enable_halo(cfd_handle *h, int side, double **buf, long long *count);
+int cfd_stage_state(cfd_handle *h, int stage, double **state);
+int cfd_rk3_stage(cfd_handle *h, int stage, double dt, double t);
+int cfd_max_wave_speeds(cfd_handle *h, double *lam);
 
 /* Library version string. */
 const char *cfd_version(void);
