@@ -26,6 +26,7 @@ data-path collective); value = all ranks' cell-steps / max rank time.
 from __future__ import annotations
 
 import argparse
+import copy
 import ctypes as C
 import json
 import os
@@ -299,17 +300,33 @@ def run_ours(args, rank, world, local_rank):
     info.device = local_rank
     info.strict = False
     info.precision = 1 if args.precision == "mixed" else 0
-    solver = zone.BlockSolver(info, periodic=True)
-    lib = solver.lib
     c, h = initial_state(dim, n, L)
+    slab = None
+    if world > 1 or args.force_slabs:
+        # one grid over the ranks: slabs along the last direction (each rank an
+        # n^dim tile of a periodic grid n^(dim-1) x (n * world)), halos by NCCL
+        from cfd_inwsl_b200 import slabs
+        ginfo = copy.deepcopy(info)
+        ginfo.iMax[dim - 1] = n * world + 1
+        ginfo.calZone[2 * (dim - 1) + 1] = L * world
+        slab = slabs.SlabRank(ginfo, periodic=True, device=local_rank)
+        solver = slab.slab.solver
+        stream = slab.stream
+    else:
+        solver = zone.BlockSolver(info, periodic=True)
+        stream = torch.cuda.Stream(device=dev)
+        _lib.check(solver.lib.cfd_set_stream(solver.h, C.c_void_p(stream.cuda_stream)), solver.h)
+    lib = solver.lib
     ncell = solver.ncell
-    stream = torch.cuda.Stream(device=dev)
-    _lib.check(lib.cfd_set_stream(solver.h, C.c_void_p(stream.cuda_stream)), solver.h)
 
     tbuf = C.c_double(0.0)
     nsteps = C.c_int(0)
 
     def run(k):
+        if slab is not None:
+            for _ in range(k):
+                slab.step(slab.max_dt(cfl))
+            return
         _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, k, C.byref(tbuf), C.byref(nsteps), None, None), solver.h)
         assert nsteps.value == k
 
@@ -386,19 +403,22 @@ def run_ours(args, rank, world, local_rank):
     hp = _lib.ptr(host)
     dts = np.zeros(1)
     lin = np.zeros(1)
-    for _ in range(2):
+    def e2e_step():
         _lib.check(lib.cfd_upload_cons(solver.h, hp), solver.h)
-        _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, 1, C.byref(tbuf), C.byref(nsteps), _lib.ptr(dts),
-                               _lib.ptr(lin)), solver.h)
+        if slab is not None:
+            slab.step(slab.max_dt(cfl))
+        else:
+            _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, 1, C.byref(tbuf), C.byref(nsteps), _lib.ptr(dts),
+                                   _lib.ptr(lin)), solver.h)
         _lib.check(lib.cfd_download_cons(solver.h, hp), solver.h)
+
+    for _ in range(2):
+        e2e_step()
     torch.cuda.synchronize()
     barrier()
     e0.record(stream)
     for _ in range(e2e_steps):
-        _lib.check(lib.cfd_upload_cons(solver.h, hp), solver.h)
-        _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, 1, C.byref(tbuf), C.byref(nsteps), _lib.ptr(dts),
-                               _lib.ptr(lin)), solver.h)
-        _lib.check(lib.cfd_download_cons(solver.h, hp), solver.h)
+        e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
@@ -407,7 +427,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the mixed FP32/FP64 form on the same workload, and both forms' accuracy
     mixed = None
-    if not args.no_mixed and args.precision == "fp64":
+    if not args.no_mixed and args.precision == "fp64" and world == 1:
         info_m = zone.Info()
         for k, v in vars(info).items():
             setattr(info_m, k, v)
@@ -432,7 +452,7 @@ def run_ours(args, rank, world, local_rank):
             mixed["l1_rho_vs_exact"] = vortex_accuracy(args.accuracy_grid, L, im, fm, cfl, local_rank)
 
     adjoint = None
-    if not args.no_adjoint and rank == 0:
+    if not args.no_adjoint and world == 1:
         adjoint = adjoint_cost(local_rank, stream)
 
     cpu = None
@@ -447,7 +467,10 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": desc, "grid": [n] * dim, "cells": ncell, "inter_method": im,
                    "flux_method": "Roe" if fm else "HLLC", "cfl": cfl, "flavour": "fast (FMA, 1e-12 parity)",
                    "l2": "inputs larger than L2: 3 state arrays + RHS of %.0f MB each" % (state_bytes / 1e6),
-                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "parallelism": (f"{world} slabs along the last direction, one per GPU, 4-row halos "
+                                   "exchanged by NCCL before every stage, dt from the ranks' maximum wave speeds")
+                                  if slab is not None else "single GPU",
+                   "global_grid": [n] * (dim - 1) + [n * world],
                    "cell_stages_per_s": 3 * value},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
@@ -457,7 +480,8 @@ def run_ours(args, rank, world, local_rank):
                      "note": "FP64-arithmetic bound path; the HBM fraction is low by construction"},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes + 16, "steps": e2e_steps,
-                "path": "cfd_upload_cons + cfd_run(1 step) + cfd_download_cons per step, pinned host buffer"},
+                "path": ("cfd_upload_cons + one step (" + ("stages with halo exchanges" if slab is not None
+                                                         else "cfd_run") + ") + cfd_download_cons per step, pinned host buffer")},
         "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -482,6 +506,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--force-slabs", action="store_true",
+                    help="run the multi-GPU slab path (halo exchange) even on one GPU (one periodic slab)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="form of the timed steps (mixed: CFD_PREC_MIXED)")
     ap.add_argument("--accuracy-grid", type=int, default=512)
@@ -508,17 +534,23 @@ def main():
         print(json.dumps(out), flush=True)
         return 0
 
-    if world > 1:
+    distributed = world > 1 or args.force_slabs
+    if distributed:
         import datetime
 
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        os.environ.setdefault("MASTER_PORT", "29511")
+        os.environ.setdefault("RANK", str(rank))
+        os.environ.setdefault("WORLD_SIZE", str(world))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
     res = run_ours(args, rank, world, local_rank)
-    if world > 1:
+    if distributed:
         import torch.distributed as dist
+        dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(res), flush=True)
