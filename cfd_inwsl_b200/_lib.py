@@ -96,6 +96,8 @@ _PROTOS = {
     "cfd_stage_state": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "cfd_rk3_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
     "cfd_max_wave_speeds": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cfd_save_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),
+    "cfd_load_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
 }
 
 

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1669,5 +1670,103 @@ int cfd_max_wave_speeds(cfd_handle *h, double *lam)
         if (d < h->dim) std::memcpy(&l, &r[1 + d], sizeof(double));
         lam[d] = l;
     }
+    return CFD_OK;
+}
+
+// ------------------------------------------------------------------ checkpoint / restart
+
+namespace {
+
+// FNV-1a, 64 bit, over the header and the payload
+uint64_t fnv1a(const void *data, size_t n, uint64_t hsh)
+{
+    const unsigned char *p = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < n; i++) {
+        hsh ^= p[i];
+        hsh *= 1099511628211ull;
+    }
+    return hsh;
+}
+
+struct CkptHeader {
+    char magic[8];         // "CFDGPUCK"
+    uint32_t version;      // 1
+    uint32_t dim;
+    int64_t n[3];
+    uint32_t nvar;
+    int32_t inter_method;
+    int32_t flux_method;
+    int32_t pad;
+    double gamma;
+    double h[3];
+    double t;
+    int64_t step;
+};
+static_assert(sizeof(CkptHeader) == 104, "checkpoint header layout");
+
+} // namespace
+
+int cfd_save_checkpoint(cfd_handle *h, const char *path, double t, long long step)
+{
+    if (!h || !path) return CFD_ERR_CONFIG;
+    const size_t n = (size_t)h->ncell * h->nv;
+    std::vector<double> cons(n);
+    int rc = cfd_download_cons(h, cons.data());
+    if (rc) return rc;
+    CkptHeader hd;
+    std::memset(&hd, 0, sizeof(hd));
+    std::memcpy(hd.magic, "CFDGPUCK", 8);
+    hd.version = 1;
+    hd.dim = (uint32_t)h->dim;
+    for (int d = 0; d < 3; d++) {
+        hd.n[d] = h->cfg.n[d];
+        hd.h[d] = h->cfg.h[d];
+    }
+    hd.nvar = (uint32_t)h->nv;
+    hd.inter_method = h->cfg.inter_method;
+    hd.flux_method = h->cfg.flux_method;
+    hd.gamma = h->cfg.gamma;
+    hd.t = t;
+    hd.step = step;
+    uint64_t sum = fnv1a(&hd, sizeof(hd), 14695981039346656037ull);
+    sum = fnv1a(cons.data(), n * sizeof(double), sum);
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(h, CFD_ERR_CONFIG, std::string("cannot open ") + path + " for writing");
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1 && std::fwrite(cons.data(), sizeof(double), n, f) == n &&
+              std::fwrite(&sum, sizeof(sum), 1, f) == 1;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(h, CFD_ERR_CONFIG, std::string("short write to ") + path);
+    return CFD_OK;
+}
+
+int cfd_load_checkpoint(cfd_handle *h, const char *path, double *t, long long *step)
+{
+    if (!h || !path) return CFD_ERR_CONFIG;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(h, CFD_ERR_CONFIG, std::string("cannot open ") + path);
+    CkptHeader hd;
+    const size_t n = (size_t)h->ncell * h->nv;
+    std::vector<double> cons(n);
+    uint64_t stored = 0;
+    bool ok = std::fread(&hd, sizeof(hd), 1, f) == 1;
+    if (ok && (std::memcmp(hd.magic, "CFDGPUCK", 8) != 0 || hd.version != 1)) {
+        std::fclose(f);
+        return fail(h, CFD_ERR_CONFIG, std::string(path) + " is not a version-1 checkpoint");
+    }
+    if (ok && (hd.dim != (uint32_t)h->dim || hd.nvar != (uint32_t)h->nv || hd.n[0] != h->cfg.n[0] ||
+               hd.n[1] != h->cfg.n[1] || hd.n[2] != h->cfg.n[2])) {
+        std::fclose(f);
+        return fail(h, CFD_ERR_CONFIG, std::string(path) + " holds a grid of another shape");
+    }
+    ok = ok && std::fread(cons.data(), sizeof(double), n, f) == n && std::fread(&stored, sizeof(stored), 1, f) == 1;
+    std::fclose(f);
+    if (!ok) return fail(h, CFD_ERR_CONFIG, std::string(path) + " is truncated");
+    uint64_t sum = fnv1a(&hd, sizeof(hd), 14695981039346656037ull);
+    sum = fnv1a(cons.data(), n * sizeof(double), sum);
+    if (sum != stored) return fail(h, CFD_ERR_CONFIG, std::string(path) + ": checksum mismatch");
+    int rc = cfd_upload_cons(h, cons.data());
+    if (rc) return rc;
+    if (t) *t = hd.t;
+    if (step) *step = hd.step;
     return CFD_OK;
 }

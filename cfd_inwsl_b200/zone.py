@@ -356,6 +356,19 @@ class BlockSolver:
                 linfs.append(linf)
         return (np.array(dts), np.array(linfs)) if record else None
 
+    # --- checkpoint / restart (cfd_save_checkpoint / cfd_load_checkpoint)
+    def save_checkpoint(self, path) -> None:
+        """Write the state with info.t and info.step."""
+        _lib.check(self.lib.cfd_save_checkpoint(self.h, str(path).encode(), float(self.info.t), int(self.info.step)),
+                   self.h)
+
+    def load_checkpoint(self, path) -> None:
+        """Read a state written by save_checkpoint; restores info.t and info.step."""
+        t, step = C.c_double(), C.c_longlong()
+        _lib.check(self.lib.cfd_load_checkpoint(self.h, str(path).encode(), C.byref(t), C.byref(step)), self.h)
+        self.info.t = t.value
+        self.info.step = step.value
+
     # --- discrete adjoint (no counterpart in the reference)
     def rhs_vjp(self, mu: np.ndarray) -> np.ndarray:
         """(dR/dU)^T mu at the current state (cfd_rhs_vjp); mu, result: AoS (ncell, nvar)."""
@@ -497,3 +510,60 @@ def prim_to_cons(prim: np.ndarray) -> np.ndarray:
     out[..., nv - 1] = p / (GAMMA - 1) + 0.5 * r * np.sum(vel * vel, axis=-1)
     return out
 
+
+
+# --------------------------------------------------------------------- checkpoint files
+CKPT_HEADER = np.dtype([("magic", "S8"), ("version", "<u4"), ("dim", "<u4"), ("n", "<i8", 3), ("nvar", "<u4"),
+                        ("inter_method", "<i4"), ("flux_method", "<i4"), ("pad", "<i4"), ("gamma", "<f8"),
+                        ("h", "<f8", 3), ("t", "<f8"), ("step", "<i8")])
+
+
+def _fnv1a(data: bytes, h: int = 14695981039346656037) -> int:
+    a = np.frombuffer(data, dtype=np.uint8)
+    for b in a.tolist():
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def read_checkpoint(path, verify: bool = True):
+    """(header dict, cons (ncell, nvar)) of a checkpoint file; raises ValueError
+    on a bad magic, version or size, and (verify=True) a bad checksum. The
+    checksum runs byte by byte in Python: pass verify=False for large files
+    (cfd_load_checkpoint always verifies)."""
+    raw = open(path, "rb").read()
+    if len(raw) < CKPT_HEADER.itemsize + 8:
+        raise ValueError("truncated checkpoint")
+    hd = np.frombuffer(raw[:CKPT_HEADER.itemsize], dtype=CKPT_HEADER)[0]
+    if hd["magic"] != b"CFDGPUCK" or hd["version"] != 1:
+        raise ValueError("not a version-1 checkpoint")
+    n = [int(x) for x in hd["n"]]
+    count = n[0] * n[1] * n[2] * int(hd["nvar"])
+    end = CKPT_HEADER.itemsize + 8 * count
+    if len(raw) != end + 8:
+        raise ValueError("checkpoint size does not match its header")
+    stored = int(np.frombuffer(raw[end:end + 8], dtype="<u8")[0])
+    if verify and _fnv1a(raw[:end]) != stored:
+        raise ValueError("checkpoint checksum mismatch")
+    cons = np.frombuffer(raw[CKPT_HEADER.itemsize:end], dtype="<f8").reshape(-1, int(hd["nvar"])).copy()
+    meta = {k: hd[k] for k in CKPT_HEADER.names if k not in ("magic", "pad")}
+    return meta, cons
+
+
+def write_checkpoint(path, info: Info, cons: np.ndarray) -> None:
+    """The file cfd_save_checkpoint writes, from the host (same layout and checksum)."""
+    hd = np.zeros((), dtype=CKPT_HEADER)
+    hd["magic"] = b"CFDGPUCK"
+    hd["version"] = 1
+    hd["dim"] = info.dim
+    n = info.icMax()
+    hd["n"] = [n[d] if d < info.dim else 1 for d in range(3)]
+    hd["nvar"] = info.nPrim()
+    hd["inter_method"] = int(info.interMethod)
+    hd["flux_method"] = int(info.fluxMethod)
+    hd["gamma"] = 1.4
+    hd["h"] = [info.geth(d) for d in range(3)]
+    hd["t"] = info.t
+    hd["step"] = info.step
+    body = hd.tobytes() + np.ascontiguousarray(cons, dtype="<f8").tobytes()
+    with open(path, "wb") as f:
+        f.write(body + np.array([_fnv1a(body)], dtype="<u8").tobytes())

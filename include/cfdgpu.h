@@ -278,6 +278,17 @@ int cfd_stage_state(cfd_handle *h, int stage, double **state);
 int cfd_rk3_stage(cfd_handle *h, int stage, double dt, double t);
 int cfd_max_wave_speeds(cfd_handle *h, double *lam);
 
+/* Binary checkpoint / restart of the state (the reference writes its output
+ * through CGNS, cgnsio.cpp:3-101, and has no restart; libcgns is not part of
+ * this library). Little-endian file: a 104-byte header (magic "CFDGPUCK",
+ * version 1, dim, n[3], nvar, inter_method, flux_method, gamma, h[3], t, step),
+ * the cons in the reference's AoS Data layout (ncell * nvar doubles), and a
+ * 64-bit FNV-1a checksum of header and payload. Loading checks the magic, the
+ * version, the grid shape and the checksum (CFD_ERR_CONFIG and a message
+ * otherwise); t and step may be NULL. */
+int cfd_save_checkpoint(cfd_handle *h, const char *path, double t, long long step);
+int cfd_load_checkpoint(cfd_handle *h, const char *path, double *t, long long *step);
+
 /* Library version string. */
 const char *cfd_version(void);
 
