@@ -162,6 +162,67 @@ __device__ __forceinline__ unsigned teno_flag_f(float q0, float q1, float q2, fl
     }
 }
 
+// The cut-off decision of a TENO family from its three smoothness measures
+// (the part of teno_flag_f after the measures), for one stencil.
+template <int FAM>
+__device__ __noinline__ unsigned teno_flag_beta(float b0, float b1, float b2, float tau, float c)
+{
+    if constexpr (FAM == FAM_TENOZ) {
+        float t0 = 1.0f + __fdividef(tau, b0 + 1e-30f), t1 = 1.0f + __fdividef(tau, b1 + 1e-30f),
+              t2 = 1.0f + __fdividef(tau, b2 + 1e-30f);
+        const float itm = __fdividef(1.0f, fmaxf(t0, fmaxf(t1, t2)));
+        t0 *= itm; t1 *= itm; t2 *= itm;
+        float m0 = t0 * t0, m1 = t1 * t1, m2 = t2 * t2;
+        m0 = m0 * m0 * m0; m1 = m1 * m1 * m1; m2 = m2 * m2 * m2;
+        const float CT = c * (m0 + m1 + m2);
+        return (m0 < CT ? 1u : 0u) + (m1 < CT ? 2u : 0u) + (m2 < CT ? 4u : 0u);
+    } else {
+        float bmin = b0;
+        if (b1 < bmin) bmin = b1;
+        if (b2 < bmin) bmin = b2;
+        const float rr = c * tau - (1.0f - c) * bmin, ll = tau * bmin;
+        return (ll < rr * b0 ? 1u : 0u) + (ll < rr * b1 ? 2u : 0u) + (ll < rr * b2 ? 4u : 0u);
+    }
+}
+
+// Both faces' stencils of one characteristic field at once, in packed FP32
+// pairs (one FFMA2 / FADD2 / FMUL2 instruction per pair): Q_i = (q_i, q_{5-i}),
+// so the left stencil q0..q4 is the .x lane of Q0..Q4 and the mirrored right
+// stencil q5..q1 the .y lane. Q3 and Q4 are Q2 and Q1 with the lanes swapped.
+template <int FAM>
+__device__ __forceinline__ void teno_flags2(float2 Q0, float2 Q1, float2 Q2, float c, float kap, unsigned &fl,
+                                            unsigned &fr)
+{
+    const float2 Q3 = make_float2(Q2.y, Q2.x), Q4 = make_float2(Q1.y, Q1.x);
+    const float2 m1 = make_float2(-1.0f, -1.0f), m2 = make_float2(-2.0f, -2.0f), m4 = make_float2(-4.0f, -4.0f),
+                 p3 = make_float2(3.0f, 3.0f), h = make_float2(0.5f, 0.5f);
+    float2 a = __ffma2_rn(m2, Q1, __fadd2_rn(Q0, Q2));
+    float2 b = __fmul2_rn(h, __ffma2_rn(p3, Q2, __ffma2_rn(m4, Q1, Q0)));
+    const float2 B0 = __ffma2_rn(a, a, __fmul2_rn(b, b));
+    a = __ffma2_rn(m2, Q2, __fadd2_rn(Q1, Q3));
+    b = __fmul2_rn(h, __ffma2_rn(m1, Q3, Q1));
+    const float2 B1 = __ffma2_rn(a, a, __fmul2_rn(b, b));
+    a = __ffma2_rn(m2, Q3, __fadd2_rn(Q2, Q4));
+    b = __fmul2_rn(h, __ffma2_rn(p3, Q2, __ffma2_rn(m4, Q3, Q4)));
+    const float2 B2 = __ffma2_rn(a, a, __fmul2_rn(b, b));
+    float2 T = __ffma2_rn(m1, B0, B2);
+    T.x = fabsf(T.x);
+    T.y = fabsf(T.y);
+    bool keep_x = false, keep_y = false;
+    if constexpr (FAM == FAM_TENOZ) {
+        // the keep-all bound of teno_z_all_kept (euler_math.cuh), per lane
+        const float2 e = make_float2(1e-30f, 1e-30f);
+        const float2 S0 = __fadd2_rn(B0, e), S1 = __fadd2_rn(B1, e), S2 = __fadd2_rn(B2, e);
+        const float2 smin = make_float2(fminf(S0.x, fminf(S1.x, S2.x)), fminf(S0.y, fminf(S1.y, S2.y)));
+        const float2 smax = make_float2(fmaxf(S0.x, fmaxf(S1.x, S2.x)), fmaxf(S0.y, fmaxf(S1.y, S2.y)));
+        const float2 rhs = __fmul2_rn(__fadd2_rn(smin, T), smax), lhs = __fmul2_rn(__fadd2_rn(smax, T), smin);
+        keep_x = rhs.x < 1e36f && lhs.x >= kap * rhs.x;
+        keep_y = rhs.y < 1e36f && lhs.y >= kap * rhs.y;
+    }
+    fl = keep_x ? 0u : teno_flag_beta<FAM>(B0.x, B1.x, B2.x, T.x, c);
+    fr = keep_y ? 0u : teno_flag_beta<FAM>(B0.y, B1.y, B2.y, T.y, c);
+}
+
 // Roe-averaged eigenvectors in FP32 from the FP64 base quantities.
 template <int NV, int AX>
 struct EigenF {
@@ -191,6 +252,17 @@ struct EigenF {
         c = sqrtf((float)(kGamma - 1) * h);
         ic = __fdividef(1.0f, c);
         ih = __fdividef(1.0f, h);
+    }
+    // entries of L that are the constant 0 (skipped in the projections)
+    static __device__ __forceinline__ constexpr bool Lzero(int k, int m)
+    {
+        constexpr int E = NV - 1;
+        if (k == 0) {
+            if (AX != 2) return m == E || (m == 1 && AX == 0) || (m == 2 && AX == 1) || (NV == 5 && m == 3);
+            return m != 0 && m != 1;
+        }
+        if (k == 4) return (AX != 2) ? (m != 0 && m != 3) : (m != 0 && m != 2);
+        return false;
     }
     __device__ __forceinline__ float L(int k, int m) const
     {
@@ -297,22 +369,33 @@ __device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &p
     const float fc = (float)icst, fk = (float)kap;
     double cl[NV], cr[NV];
     if constexpr (FAM == FAM_TENOZ || FAM == FAM_TENOCONG) {
+        // increments of the stencil pairs (0, 5), (1, 4), (2, 3); cell 2's is 0
+        float2 D[3][NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+            D[0][m] = make_float2(d[0][m], d[5][m]);
+            D[1][m] = make_float2(d[1][m], d[4][m]);
+            D[2][m] = make_float2(0.0f, d[3][m]);
+        }
         unsigned fL = 0, fR = 0;
 #pragma unroll
         for (int k = 0; k < NV; k++) {
-            float l[NV];
+            float2 Q[3];
 #pragma unroll
-            for (int m = 0; m < NV; m++) l[m] = eb.L(k, m);
-            float q[6];
+            for (int i = 0; i < 3; i++) {
+                float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-            for (int j = 0; j < 6; j++) {
-                float a = 0.0f;
-#pragma unroll
-                for (int m = 0; m < NV; m++) a += d[j][m] * l[m];
-                q[j] = a;
+                for (int m = 0; m < NV; m++) {
+                    if (EigenF<NV, AX>::Lzero(k, m)) continue;
+                    const float l = eb.L(k, m);
+                    acc = __ffma2_rn(make_float2(l, l), D[i][m], acc);
+                }
+                Q[i] = acc;
             }
-            fL |= teno_flag_f<FAM>(q[0], q[1], q[2], q[3], q[4], fc, fk) << (3 * k);
-            fR |= teno_flag_f<FAM>(q[5], q[4], q[3], q[2], q[1], fc, fk) << (3 * k);
+            unsigned fl, fr;
+            teno_flags2<FAM>(Q[0], Q[1], Q[2], fc, fk, fl, fr);
+            fL |= fl << (3 * k);
+            fR |= fr << (3 * k);
         }
         // one stencil in every field: R L = I, apply it to the cons directly
         constexpr unsigned kRep = (NV == 4) ? 01111u : 011111u;
