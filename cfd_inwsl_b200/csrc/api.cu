@@ -182,8 +182,8 @@ __global__ void eval_face_kernel(const double *prims6, int n, double c, double k
                     hi[j][v] = (float)cs6[j][v];
                     lo[j][v] = (float)(cs6[j][v] - (double)hi[j][v]);
                 }
-            auto inc = [&](int j, int v) { return (hi[j][v] - hi[2][v]) + (lo[j][v] - lo[2][v]); };
-            cfd::reconstruct_face_mixed<NV, AX, FAM>(cs, pr, inc, c, kap, fl, fr);
+            auto hl = [&](int j, int v) { return make_float2(hi[j][v], lo[j][v]); };
+            cfd::reconstruct_face_mixed<NV, AX, FAM>(cs, pr, hl, c, kap, fl, fr);
         } else {
             cfd::reconstruct_face_stream<NV, AX, FAM>(cs, pr, c, kap, fl, fr);
         }

@@ -345,8 +345,9 @@ __device__ __noinline__ void recon_flags64(const CS &cs, const PR &pr, unsigned 
     }
 }
 
-// cs(j, v) / pr(j, v): FP64 cons and prim of stencil cell j; inc(j, v): FP32
-// cons(j, v) - cons(2, v). Writes FP64 face prims.
+// cs(j, v) / pr(j, v): FP64 cons and prim of stencil cell j; hl(j, v): the FP32
+// hi/lo split (hi, lo) of cons(j, v), whose differences to cell 2 give the FP32
+// increments. Writes FP64 face prims.
 //
 // Continuous-weight families: the face increment is split as
 // U_face - U_2 = Lin(dU) + R (NL(q) - Lin(q)), q = L dU, which equals
@@ -356,26 +357,24 @@ __device__ __noinline__ void recon_flags64(const CS &cs, const PR &pr, unsigned 
 // through the FP32 eigenvectors, whose R L differs from the identity by about
 // 1e-7 times their condition number (large at low Mach number, where
 // h = c^2/(gamma-1) dominates).
-template <int NV, int AX, int FAM, class CS, class PR, class INC>
-__device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &pr, const INC &inc, double icst,
+template <int NV, int AX, int FAM, class CS, class PR, class HL>
+__device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &pr, const HL &hl, double icst,
                                                        double kap, double *fl, double *fr)
 {
     const EigenF<NV, AX> eb(pr);
-    float d[6][NV];
-#pragma unroll
-    for (int j = 0; j < 6; j++)
-#pragma unroll
-        for (int m = 0; m < NV; m++) d[j][m] = (j == 2) ? 0.0f : inc(j, m);
     const float fc = (float)icst, fk = (float)kap;
     double cl[NV], cr[NV];
     if constexpr (FAM == FAM_TENOZ || FAM == FAM_TENOCONG) {
-        // increments of the stencil pairs (0, 5), (1, 4), (2, 3); cell 2's is 0
+        // increments of the stencil pairs (0, 5), (1, 4), (2, 3), packed; cell 2's is 0
         float2 D[3][NV];
+        const float2 m1 = make_float2(-1.0f, -1.0f);
 #pragma unroll
         for (int m = 0; m < NV; m++) {
-            D[0][m] = make_float2(d[0][m], d[5][m]);
-            D[1][m] = make_float2(d[1][m], d[4][m]);
-            D[2][m] = make_float2(0.0f, d[3][m]);
+            const float2 c2 = hl(2, m), c0 = hl(0, m), c5 = hl(5, m), c1 = hl(1, m), c4 = hl(4, m), c3 = hl(3, m);
+            const float2 H2 = make_float2(c2.x, c2.x), L2 = make_float2(c2.y, c2.y);
+            D[0][m] = __fadd2_rn(__ffma2_rn(m1, H2, make_float2(c0.x, c5.x)), __ffma2_rn(m1, L2, make_float2(c0.y, c5.y)));
+            D[1][m] = __fadd2_rn(__ffma2_rn(m1, H2, make_float2(c1.x, c4.x)), __ffma2_rn(m1, L2, make_float2(c1.y, c4.y)));
+            D[2][m] = make_float2(0.0f, (c3.x - c2.x) + (c3.y - c2.y));
         }
         unsigned fL = 0, fR = 0;
 #pragma unroll
@@ -410,6 +409,14 @@ __device__ __forceinline__ void reconstruct_face_mixed(const CS &cs, const PR &p
             recon_flags64<NV, AX>(cs, pr, fL, fR, cl, cr);
         }
     } else {
+        float d[6][NV];
+#pragma unroll
+        for (int j = 0; j < 6; j++)
+#pragma unroll
+            for (int m = 0; m < NV; m++) {
+                const float2 cj = hl(j, m), c2 = hl(2, m);
+                d[j][m] = (j == 2) ? 0.0f : (cj.x - c2.x) + (cj.y - c2.y);
+            }
         float dl[NV], dr[NV];
 #pragma unroll
         for (int i = 0; i < NV; i++) {

@@ -152,8 +152,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     double *sp = smem;                   // [NV][W][LSP] prim
     double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue)
     double *sf = sc + NV * W * LSP;      // [NV][W][LSF] face flux
-    float *shi = reinterpret_cast<float *>(sf + NV * W * LSF);  // mixed form: [NV][W][LSP] (float)cons
-    float *slo = shi + NV * W * LSP;                            //             [NV][W][LSP] cons - hi
+    // mixed form: [NV][W][LSP] (hi, lo) = ((float)cons, (float)(cons - hi))
+    float2 *shl = reinterpret_cast<float2 *>(sf + NV * W * LSF);
     // staging: [0] next chunk's cons, [1] rhs, [2] U^0, [3] U^k; [NV][NT] each
     double *stg = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + SH::SMEM_RINGS);
     constexpr bool PF = SH::PF, PF_EPI = SH::PF_EPI;
@@ -219,8 +219,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             sc[(v * W + l) * LSP + slot] = cs[v];
             if constexpr (PREC == 1) {
                 const float hi = (float)cs[v];
-                shi[(v * W + l) * LSP + slot] = hi;
-                slo[(v * W + l) * LSP + slot] = (float)(cs[v] - (double)hi);
+                shl[(v * W + l) * LSP + slot] = make_float2(hi, (float)(cs[v] - (double)hi));
             }
         }
     };
@@ -247,14 +246,12 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             auto csacc = [&](int m, int v) { return scl[v * W * LSP + slot[m]]; };
             auto pracc = [&](int m, int v) { return spl[v * W * LSP + slot[m]]; };
             if constexpr (PREC == 1) {
-                const float *hil = shi + l * LSP, *lol = slo + l * LSP;
-                // cons(j) - cons(2) in FP32: the hi parts of neighbouring cells
-                // subtract exactly wherever the increment is small
-                auto incacc = [&](int m, int v) {
-                    const int a = v * W * LSP;
-                    return (hil[a + slot[m]] - hil[a + slot[2]]) + (lol[a + slot[m]] - lol[a + slot[2]]);
+                const float2 *hll = shl + l * LSP;
+                // the FP32 hi/lo split of each stencil cell's cons
+                auto hlacc = [&](int m, int v) {
+                    return hll[v * W * LSP + slot[m]];
                 };
-                reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, incacc, p.icst, p.icst_k, fl, fr);
+                reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, hlacc, p.icst, p.icst_k, fl, fr);
             } else {
                 reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, p.icst_k, fl, fr);
             }
