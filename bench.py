@@ -282,6 +282,49 @@ def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
             "J": J, "grad_l2": float(np.linalg.norm(out["g"]))}
 
 
+def batch_throughput(device, stream, ncases=256, steps=20, seed=0):
+    """Batched configuration: 256 independent 2D Riemann problems on [0,1]^2,
+    N = round(2^U(7,10)) cells per side (seeded), quadrant states rho ~
+    U[0.1,2], p ~ U[0.05,2], u, v ~ U[-1,1], WCNS5 + HLLC, CFL 0.5, per-case dt,
+    transmissive boundaries, advanced together in one persistent launch per
+    sweep. Timed: `steps` steps of every case (cfd_batch_run with max_steps),
+    CUDA events on the batch's stream, after 3 warm-up steps."""
+    import torch
+    from cfd_inwsl_b200 import _lib, cases, zone
+    rng = np.random.default_rng(seed)
+    sizes = [int(round(2 ** rng.uniform(7, 10))) for _ in range(ncases)]
+    infos = []
+    for n in sizes:
+        info = zone.Info()
+        info.dim = 2
+        info.iMax = [n + 1, n + 1, 1]
+        info.calZone = [0, 1, 0, 1, 0, 0]
+        info.interMethod = 2
+        info.fluxMethod = 0
+        info.CFL = 0.5
+        info.nCase = 0
+        info.device = device
+        infos.append(info)
+    b = zone.BlockBatch(infos)
+    _lib.check(b.lib.cfd_batch_set_stream(b.h, C.c_void_p(stream.cuda_stream)))
+    for i, n in enumerate(sizes):
+        b.set_cons(i, cases.riemann_quadrants(n, rng))
+    b.run(0.25, end_step=1, max_steps=3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _, ns = b.run(0.25, end_step=1, max_steps=steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cell_steps = float(sum(n * n * int(k) for n, k in zip(sizes, ns)))
+    b.close()
+    return {"config": f"{ncases} cases, N = round(2^U(7,10)) (seeded, {min(sizes)}..{max(sizes)}), "
+                      "WCNS5 + HLLC, CFL 0.5, transmissive, per-case dt",
+            "cells": int(sum(n * n for n in sizes)), "steps_per_case": steps, "ms": ms,
+            "value": cell_steps / (ms / 1e3), "unit": "cell-steps/s"}
+
+
 # --------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -454,6 +497,9 @@ def run_ours(args, rank, world, local_rank):
     adjoint = None
     if not args.no_adjoint and world == 1:
         adjoint = adjoint_cost(local_rank, stream)
+    batch = None
+    if not args.no_batch and world == 1:
+        batch = batch_throughput(local_rank, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -489,6 +535,8 @@ def run_ours(args, rank, world, local_rank):
         result["mixed"] = mixed
     if adjoint is not None:
         result["adjoint"] = adjoint
+    if batch is not None:
+        result["batch"] = batch
     if cpu is not None:
         result["cpu_baseline"] = cpu
     solver.close()
@@ -506,6 +554,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--force-slabs", action="store_true",
                     help="run the multi-GPU slab path (halo exchange) even on one GPU (one periodic slab)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],

@@ -11,8 +11,14 @@ namespace cfd {
 #ifndef CFD_XW
 #define CFD_XW 4
 #endif
+#ifndef CFD_YS
+#define CFD_YS 8
+#endif
+#ifndef CFD_YW
+#define CFD_YW 32
+#endif
 constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
-constexpr int kYS = 8, kYW = 32;           // along y and z
+constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
 constexpr int k1S = 128, k1W = 1;          // 1D
 
 
