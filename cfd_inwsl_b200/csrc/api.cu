@@ -1159,6 +1159,9 @@ struct cfd_batch {
     SweepParams *d_params = nullptr;
     long long *d_tile_start = nullptr;  // [dim][ncases + 1]
     std::vector<long long> tile_total;
+    // work-list order: cases by decreasing cell count, so that the persistent
+    // CTAs take the longest tiles first and the tail holds the short ones
+    std::vector<int> order;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     unsigned long long launches = 0;
@@ -1283,13 +1286,16 @@ int cfd_batch_create(const cfd_config *cfgs, int ncases, cfd_batch **out)
     size_t np = (size_t)9 * b->dim * ncases;
     b->params_host.resize(np);
     if ((e = cudaMalloc(&b->d_params, sizeof(SweepParams) * np)) != cudaSuccess) return bail(e);
+    b->order.resize(ncases);
+    for (int c = 0; c < ncases; c++) b->order[c] = c;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->h[x]->ncell > b->h[y]->ncell; });
     std::vector<long long> ts((size_t)b->dim * (ncases + 1));
     b->tile_total.assign(b->dim, 0);
     for (int d = 0; d < b->dim; d++) {
         long long acc = 0;
-        for (int c = 0; c < ncases; c++) {
-            ts[(size_t)d * (ncases + 1) + c] = acc;
-            acc += cfd::sweep_tile_count(b->nv, d, base_params(b->h[c], d));
+        for (int i = 0; i < ncases; i++) {
+            ts[(size_t)d * (ncases + 1) + i] = acc;
+            acc += cfd::sweep_tile_count(b->nv, d, base_params(b->h[b->order[i]], d));
         }
         ts[(size_t)d * (ncases + 1) + ncases] = acc;
         b->tile_total[d] = acc;
@@ -1356,9 +1362,9 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
     for (int slot = 0; slot < 3; slot++)
         for (int stage = 1; stage <= 3; stage++)
             for (int d = 0; d < b->dim; d++)
-                for (int c = 0; c < b->ncases; c++)
-                    b->params_host[(size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases + c] =
-                        batch_params(b, c, slot, stage, d);
+                for (int i = 0; i < b->ncases; i++)
+                    b->params_host[(size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases + i] =
+                        batch_params(b, b->order[i], slot, stage, d);
     CFD_BCUDA(b, cudaMemcpyAsync(b->d_params, b->params_host.data(), sizeof(SweepParams) * b->params_host.size(),
                                  cudaMemcpyHostToDevice, b->stream));
     for (int c = 0; c < b->ncases; c++) {
