@@ -23,7 +23,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libcfdgpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FAMILIES = [0, 1, 2, 3, 4]
+FAMILIES = [0, 1, 2, 3, 4, 5]
 NVS = [3, 4, 5]
 
 

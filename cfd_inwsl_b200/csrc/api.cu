@@ -220,13 +220,33 @@ InterMap map_inter_method(int m, int dim)
     case 9: return {cfd::FAM_TENOCONG, 0.23050581003334941, true};   // WCNS5CONGZCT4 -> Teno5_CongZCT4
     case 10:
         // WCNS5CONGZCT7: Teno5_CongZCT7 in 2D, but Teno5_CongAA in 1D (solverType.cpp:248-250).
-        if (dim == 1) return {0, 0.0, false};
+        if (dim == 1) return {cfd::FAM_RESEARCH, (double)cfd::RV_CONGAA, true};
         return {cfd::FAM_TENOCONG, 0.072892337360747711, true};
+    // the research variants (solverType.cpp:262-388, 1D; 445-576, 2D)
+    case 17: return {cfd::FAM_RESEARCH, (double)cfd::RV_TCNSN, true};      // whfTCNSN
+    case 18: return {cfd::FAM_RESEARCH, (double)cfd::RV_TCNSN_A, true};    // whfTCNSNA
+    case 19: return {cfd::FAM_RESEARCH, (double)cfd::RV_TCNSN_AS, true};   // whfTCNSNAS
+    case 20: return {cfd::FAM_RESEARCH, (double)cfd::RV_TCNSN_S, true};    // whfTCNSNS
+    case 21: return {cfd::FAM_RESEARCH, (double)cfd::RV_TCNSN_LAD, true};  // whfTCNSNLAD
+    case 24: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_S, true};       // whfAITCNSNS
+    case 25: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_A, true};       // whfAITCNSNA
+    case 26: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_AS1, true};     // whfAITCNSNAS_1
+    case 27: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_AS2, true};     // whfAITCNSNAS_2
+    case 28: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_LADS, true};    // whfAITCNSNLADS
+    case 29: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_AZS, true};     // whfAITCNSNAZS
+    case 30: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_ASF1, true};    // whfAITCNSNmyASF002_1
+    case 31: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_ASF2, true};    // whfAITCNSNmyASF002_2
+    case 32: return {cfd::FAM_RESEARCH, (double)cfd::RV_AI_ASFAI1, true};  // whfAITCNSNmyASF002_ai1
+    case 33: return {cfd::FAM_RESEARCH, (double)cfd::RV_ZYC, true};        // whfzycTCNSNmyASF002_1
+    case 34: return {cfd::FAM_RESEARCH, (double)cfd::RV_COMPARE, true};    // whfCOMPARE
+    case 36: return {cfd::FAM_RESEARCH, (double)cfd::RV_NEW_A, true};      // new_WHFTCNSA
+    case 38: return {cfd::FAM_RESEARCH, (double)cfd::RV_F203, true};       // new_WHFTCNSASF203_NoS
+    case 39: return {cfd::FAM_RESEARCH, (double)cfd::RV_F202, true};       // new_WHFTCNSASF202_NoS
     case 15: return {cfd::FAM_MUSCL, 0.0, true};                // MUCSLIN5 -> musclIn5
     case 0: case 1: case 4: case 5: case 6: case 7: case 14: case 16:
         return {cfd::FAM_WCNS5, 0.0, true};                     // selector default: weno5_JSchen
     default:
-        return {0, 0.0, false};                                 // TENO-A/AS research variants
+        return {0, 0.0, false};                                 // not an InterMethod
     }
 }
 
@@ -641,6 +661,8 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     // the mixed form reconstructs in FP32 (multi-dimensional fast flavour only);
     // the strict flavour is the bit-for-bit FP64 build
     if (cfg->precision == CFD_PREC_MIXED && (cfg->dim < 2 || cfg->strict)) return CFD_ERR_UNSUPPORTED;
+    if (cfg->precision == CFD_PREC_MIXED && map_inter_method(cfg->inter_method, cfg->dim).fam == cfd::FAM_RESEARCH)
+        return CFD_ERR_UNSUPPORTED;  // the research variants have no FP32 decision form
     if (cfg->source_type != 0 && !(cfg->source_type == 1 && cfg->dim == 2)) return CFD_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) {
         if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
@@ -983,6 +1005,7 @@ int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double
     case cfd::FAM_WENOZ: eval_inter5_kernel<cfd::FAM_WENOZ><<<g, 256>>>(dq, n, im.c, kap, dout); break;
     case cfd::FAM_TENOZ: eval_inter5_kernel<cfd::FAM_TENOZ><<<g, 256>>>(dq, n, im.c, kap, dout); break;
     case cfd::FAM_TENOCONG: eval_inter5_kernel<cfd::FAM_TENOCONG><<<g, 256>>>(dq, n, im.c, kap, dout); break;
+    case cfd::FAM_RESEARCH: eval_inter5_kernel<cfd::FAM_RESEARCH><<<g, 256>>>(dq, n, im.c, kap, dout); break;
     default: eval_inter5_kernel<cfd::FAM_MUSCL><<<g, 256>>>(dq, n, im.c, kap, dout); break;
     }
     cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
@@ -1025,7 +1048,7 @@ extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, c
     if (precision == 1 && dim == 1) return CFD_ERR_UNSUPPORTED;
     InterMap im = map_inter_method(inter_method, dim);
     const double kap = (im.fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(im.c) : 0.0;
-    if (!im.ok) return CFD_ERR_UNSUPPORTED;
+    if (!im.ok || (precision == 1 && im.fam == cfd::FAM_RESEARCH)) return CFD_ERR_UNSUPPORTED;
     if (n <= 0) return CFD_OK;
     int nv = dim + 2;
     double *din = nullptr, *dout = nullptr;
@@ -1039,13 +1062,13 @@ extern "C" int cfd_eval_face(int dim, int ax, int inter_method, int precision, c
     bool launched = false;
 #define CFD_EFACE(NV, AX, F)                                                                                  \
     if (!launched && nv == NV && ax == AX && im.fam == F) {                                                   \
-        if (precision == 1) eval_face_kernel<NV, AX, F, (NV >= 4 ? 1 : 0)><<<g, 128>>>(din, n, im.c, kap, dout); \
+        if (precision == 1) eval_face_kernel<NV, AX, F, (NV >= 4 && F != 5 ? 1 : 0)><<<g, 128>>>(din, n, im.c, kap, dout); \
         else eval_face_kernel<NV, AX, F, 0><<<g, 128>>>(din, n, im.c, kap, dout);                             \
         launched = true;                                                                                      \
     }
 #define CFD_EFACE_F(F) CFD_EFACE(3, 0, F) CFD_EFACE(4, 0, F) CFD_EFACE(4, 1, F) CFD_EFACE(5, 0, F) \
                        CFD_EFACE(5, 1, F) CFD_EFACE(5, 2, F)
-    CFD_EFACE_F(0) CFD_EFACE_F(1) CFD_EFACE_F(2) CFD_EFACE_F(3) CFD_EFACE_F(4)
+    CFD_EFACE_F(0) CFD_EFACE_F(1) CFD_EFACE_F(2) CFD_EFACE_F(3) CFD_EFACE_F(4) CFD_EFACE_F(5)
 #undef CFD_EFACE_F
 #undef CFD_EFACE
     cudaError_t e = cudaMemcpy(out, dout, sizeof(double) * 2 * nv * n, cudaMemcpyDeviceToHost);
@@ -1072,6 +1095,7 @@ extern "C" int cfd_accuracy_test(int inter_method, int n, double h, const double
     case cfd::FAM_WENOZ: accuracy_kernel<cfd::FAM_WENOZ><<<g, 128>>>(dq, n, h, im.c, dout); break;
     case cfd::FAM_TENOZ: accuracy_kernel<cfd::FAM_TENOZ><<<g, 128>>>(dq, n, h, im.c, dout); break;
     case cfd::FAM_TENOCONG: accuracy_kernel<cfd::FAM_TENOCONG><<<g, 128>>>(dq, n, h, im.c, dout); break;
+    case cfd::FAM_RESEARCH: accuracy_kernel<cfd::FAM_RESEARCH><<<g, 128>>>(dq, n, h, im.c, dout); break;
     default: accuracy_kernel<cfd::FAM_MUSCL><<<g, 128>>>(dq, n, h, im.c, dout); break;
     }
     cudaError_t e = cudaMemcpy(dqdx, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);

@@ -128,6 +128,34 @@ enum InterFamily : int {
                      //   (c = cutoff factor 1e-5, 1e-4, 1e-7, 1e-5, 1e-10, 1e-5)
     FAM_TENOCONG = 3,// Teno5_CongZ / CongZCT4 / CongZCT7 / new_Teno5_CongZ (c = CT)
     FAM_MUSCL = 4,   // musclIn5 (minmod on q1..q3)        interScheme.hpp:1386-1406
+    FAM_RESEARCH = 5,// the adaptive-cut-off TENO research variants (whf_*, TCNS_AS_*, Teno5_CongAA),
+                     //   interScheme.hpp:304-382, 1458-1762, 1901-4209 (c = the variant, ResearchVariant)
+};
+
+// The research variants of the selector (InterMethod entries 17-21, 24-34, 36,
+// 38, 39, and entry 10 in 1D). All of them interpolate with the eight fixed
+// TENO stencils of teno_select and differ only in the cut-off decision.
+enum ResearchVariant : int {
+    RV_TCNSN = 0,     // whf_TcnsN              interScheme.hpp:1458-1517
+    RV_TCNSN_A,       // whf_TcnsN_A            interScheme.hpp:3253-3361
+    RV_TCNSN_AS,      // whf_TcnsN_AS           interScheme.hpp:1581-1679
+    RV_TCNSN_S,       // whf_TcnsN_S            interScheme.hpp:1519-1579
+    RV_TCNSN_LAD,     // whf_TcnsN_LAD          interScheme.hpp:1681-1761
+    RV_AI_S,          // whf_ai_TcnsN_S_1       interScheme.hpp:1901-1994
+    RV_AI_A,          // whf_ai_TcnsN_A_2       interScheme.hpp:2216-2327
+    RV_AI_AS1,        // whf_ai_TcnsN_AS_1      interScheme.hpp:2329-2422
+    RV_AI_AS2,        // whf_ai_TcnsN_AS_2      interScheme.hpp:2424-2510
+    RV_AI_LADS,       // whf_ai_TcnsN_LADS_yuanbao interScheme.hpp:2512-2645
+    RV_AI_AZS,        // whf_ai_TcnsN_AZS_yuanbao  interScheme.hpp:2862-2934
+    RV_AI_ASF1,       // whf_ai_TcnsN_myASF002_1   interScheme.hpp:2936-3027
+    RV_AI_ASF2,       // whf_ai_TcnsN_myASF002_2   interScheme.hpp:3029-3112
+    RV_AI_ASFAI1,     // whf_ai_TcnsN_myASF002_ai1 interScheme.hpp:3114-3241
+    RV_ZYC,           // whf_zyc_TcnsN_myASF002_1  interScheme.hpp:3363-3470
+    RV_COMPARE,       // whf_TcnsN_COMPARE      interScheme.hpp:3472-3726
+    RV_NEW_A,         // new_whf_TCNS_A         interScheme.hpp:3863-3982
+    RV_F203,          // whf_TCNS_AS_myF203_NoS interScheme.hpp:3984-4091
+    RV_F202,          // whf_TCNS_AS_myF202_NoS interScheme.hpp:4093-4209
+    RV_CONGAA,        // Teno5_CongAA (1D WCNS5CONGZCT7) interScheme.hpp:304-382
 };
 
 // The TENO-Z cut-off flag (Teno5_Z, interScheme.hpp:384-452) from the three
@@ -173,6 +201,209 @@ unsigned teno_z_flag(double b0, double b1, double b2, double tau, double c)
     if (b1 < CT) flag += 2;
     if (b2 < CT) flag += 4;
     return flag;
+}
+
+// The cut-off flag of a research variant (bit k set = stencil k cut), in the
+// reference's operation order wherever the variant uses only + - * / floor
+// min max (bitwise parity); variants that call pow() agree to pow's rounding
+// (libm's and CUDA's pow differ by up to a few ulps, which can flip a decision
+// only at its threshold). Out of line on the device: one copy serves the eight
+// interpolations of a face.
+#if defined(__CUDACC__)
+static __host__ __device__ __noinline__
+#else
+static inline
+#endif
+unsigned research_flag(int variant, double q0, double q1, double q2, double q3, double q4)
+{
+    double b0, b1, b2;
+    smoothness3(q0, q1, q2, q3, q4, b0, b1, b2);
+    const double tau = fabs(b2 - b0);
+    // the smallest measure (std::min over {beta0, beta1, beta2}, or its
+    // std::min_element: the same value)
+    double bmin = b0;
+    if (b1 < bmin) bmin = b1;
+    if (b2 < bmin) bmin = b2;
+    // gamma-type measures (1 + tau / (beta_k + 1e-40))^6 by pow, and by squares and cubes
+    auto gpow = [&](double b) { return pow(1.0 + tau / (b + 1e-40), 6.0); };
+    auto gsq = [&](double b) {
+        double g = 1.0 + tau / (b + 1e-40);
+        g = g * g;
+        return g * g * g;
+    };
+    // cut when gamma_k / sum < CT
+    auto cut_ratio = [](double g0, double g1, double g2, double CT) {
+        const double s = g0 + g1 + g2;
+        return (g0 / s < CT ? 1u : 0u) + (g1 / s < CT ? 2u : 0u) + (g2 / s < CT ? 4u : 0u);
+    };
+    // cut when gamma_k < CT * sum
+    auto cut_prod = [](double g0, double g1, double g2, double CT) {
+        const double rr = CT * (g0 + g1 + g2);
+        return (g0 < rr ? 1u : 0u) + (g1 < rr ? 2u : 0u) + (g2 < rr ? 4u : 0u);
+    };
+    // cut when beta_k tau < (CTp tau - (1 - CTp) beta_k) beta_min (whf_TcnsN_S form)
+    auto cut_cross_a = [&](double CTp) {
+        unsigned f = 0;
+        if (b0 * tau < (CTp * tau - 1.0 * (1.0 - CTp) * b0) * bmin) f += 1;
+        if (b1 * tau < (CTp * tau - 1.0 * (1.0 - CTp) * b1) * bmin) f += 2;
+        if (b2 * tau < (CTp * tau - 1.0 * (1.0 - CTp) * b2) * bmin) f += 4;
+        return f;
+    };
+    // cut when beta_min tau < (CTp tau - (1 - CTp) beta_min) beta_k (the ai_* form)
+    auto cut_cross_b = [&](double CTp) {
+        const double th = CTp * tau - 1.0 * (1.0 - CTp) * bmin;
+        const double l = bmin * tau;
+        return (l < th * b0 ? 1u : 0u) + (l < th * b1 ? 2u : 0u) + (l < th * b2 ? 4u : 0u);
+    };
+    // cut when tau beta_min < (CT tau - (1 - CT) beta_min) beta_k (Teno5_CongZ form)
+    auto cut_cong = [&](double CT) {
+        const double rr = CT * tau - (1 - CT) * bmin, ll = tau * bmin;
+        return (ll < rr * b0 ? 1u : 0u) + (ll < rr * b1 ? 2u : 0u) + (ll < rr * b2 ? 4u : 0u);
+    };
+    auto ctp_of = [](double CT) { return pow(1.5 * CT / (1.0 - CT), 1.0 / 6.0); };
+    // eta on neighbouring differences dq(k+1/2) = q_{k+1} - q_k of the stencil (ai_* variants)
+    constexpr double kEpsA = (0.9 * 0.24) / (1 - 0.9 * 0.24) * 1e-3 * 1e-3;
+    auto eta_ai = [&](double epsA) {
+        const double dm3 = q1 - q0, dm1 = q2 - q1, dp1 = q3 - q2, dp3 = q4 - q3;
+        const double e0 = (fabs(2 * dm1 * dm3) + epsA) / (dm1 * dm1 + dm3 * dm3 + epsA);
+        const double e1 = (fabs(2 * dp1 * dm1) + epsA) / (dp1 * dp1 + dm1 * dm1 + epsA);
+        const double e2 = (fabs(2 * dp3 * dp1) + epsA) / (dp3 * dp3 + dp1 * dp1 + epsA);
+        double m = e0;
+        if (e1 < m) m = e1;
+        if (e2 < m) m = e2;
+        return m;
+    };
+    // eta on the stencil values themselves (whf_TcnsN_AS, Teno5_CongAA)
+    auto eta_raw = [&]() {
+        auto e = [&](double a, double b, double c) {
+            const double x1 = (fabs(2 * b * a) + kEpsA) / (b * b + a * a + kEpsA);
+            const double x2 = (fabs(2 * c * b) + kEpsA) / (c * c + b * b + kEpsA);
+            return (x2 < x1) ? x2 : x1;
+        };
+        const double e0 = e(q0, q1, q2), e1 = e(q1, q2, q3), e2 = e(q2, q3, q4);
+        double m = e0;
+        if (e1 < m) m = e1;
+        if (e2 < m) m = e2;
+        return m;
+    };
+    // CT of the A-type variants from the switch on floor(10 - 5 (1 - g))
+    auto ct_switch = [](int beta_A) {
+        switch (beta_A) {
+        case 5: return 1e-5;
+        case 6: return 1e-6;
+        case 7: return 1e-7;
+        case 8: return 1e-8;
+        case 9: return 1e-9;
+        default: return 1e-10;
+        }
+    };
+    switch (variant) {
+    case RV_TCNSN:
+        return cut_ratio(gpow(b0), gpow(b1), gpow(b2), 1e-10);
+    case RV_TCNSN_S:
+        return cut_cross_a(ctp_of(1e-5));
+    case RV_TCNSN_AS: {
+        const double m = 1.0 - fmin(1.0, eta_raw() / 0.24);
+        const double g = pow(1 - m, 4.0) * (1 + 4 * m);
+        const int bA = (int)floor(10.0 - 5.0 * (1 - g));
+        return cut_cross_a(ctp_of(pow(10.0, (double)-bA)));
+    }
+    case RV_TCNSN_LAD: {
+        const double c0 = tau / (b0 + 1e-40), c1 = tau / (b1 + 1e-40), c2 = tau / (b2 + 1e-40);
+        const double cmax = fmax(c0, fmax(c1, c2));
+        const double theta = 1.0 / (1.0 + cmax / 10.0);
+        int m = 4 + (int)floor(theta * 6);
+        m = m < 4 ? 4 : (m > 10 ? 10 : m);
+        const double tab[7] = {1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9, 1e-10};
+        return cut_ratio(gpow(b0), gpow(b1), gpow(b2), tab[m - 4]);
+    }
+    case RV_TCNSN_A: case RV_COMPARE: case RV_NEW_A: {
+        const double epsA = (variant == RV_COMPARE) ? kEpsA : 2.7551 * 1e-7;
+        const double d0 = q0 - q1, d1 = q1 - q2, d2 = q2 - q3, d3 = q3 - q4;
+        double e0, e1, e2;
+        if (variant == RV_NEW_A) {
+            e0 = (fabs(2.0 * d0 * d1) + epsA) / (d0 * d0 + d1 * d1 + epsA);
+            e1 = (fabs(2.0 * d1 * d2) + epsA) / (d1 * d1 + d2 * d2 + epsA);
+            e2 = (fabs(2.0 * d2 * d3) + epsA) / (d2 * d2 + d3 * d3 + epsA);
+        } else {
+            e0 = (fabs(2.0 * d0 * d2) + epsA) / (d0 * d0 + d2 * d2 + epsA);
+            e1 = (fabs(2.0 * d1 * d3) + epsA) / (d1 * d1 + d3 * d3 + epsA);
+            e2 = (fabs(2.0 * d2 * d1) + epsA) / (d2 * d2 + d1 * d1 + epsA);
+        }
+        double emin = e0;
+        if (e1 < emin) emin = e1;
+        if (e2 < emin) emin = e2;
+        double g;
+        if (variant == RV_NEW_A) {
+            const double mn = fmin(1.0, 4.1666667 * emin);
+            g = mn * mn * mn * mn * (5.0 - 4 * mn);
+        } else {
+            const double m = 1.0 - fmin(1.0, variant == RV_COMPARE ? emin / 0.24 : 4.1666667 * emin);
+            g = (1 - m) * (1 - m) * (1 - m) * (1 - m) * (1 + 4 * m);
+        }
+        const int bA = (int)floor(10.0 - 5.0 * (1 - g));
+        return cut_prod(gsq(b0), gsq(b1), gsq(b2), ct_switch(bA));
+    }
+    case RV_AI_S:
+        return cut_cross_b(ctp_of(1e-5));
+    case RV_AI_A: {
+        const double m = 1.0 - fmin(1.0, eta_ai(kEpsA) / 0.24);
+        const double g = pow(1 - m, 4.0) * (1 + 4 * m);
+        const double CT = pow(10.0, -floor(10.0 - 5.0 * (1 - g)));
+        return cut_ratio(gpow(b0), gpow(b1), gpow(b2), CT);
+    }
+    case RV_AI_AS1: case RV_AI_AS2: {
+        const double m = 1.0 - fmin(1.0, eta_ai(kEpsA) / 0.24);
+        const double g = pow(1.0 - m, 4.0) * (1.0 + 4.0 * m);
+        const double CT = pow(10.0, -floor(10.0 - 5.0 * (1.0 - g)));
+        return cut_cross_b(ctp_of(CT));
+    }
+    case RV_AI_LADS: {
+        const double c0 = tau / (b0 + 1e-40), c1 = tau / (b1 + 1e-40), c2 = tau / (b2 + 1e-40);
+        const double cmax = fmax(c0, fmax(c1, c2));
+        const double theta = 1.0 / (1.0 + cmax / 10.0);
+        const int m = 5 + (int)floor(theta * 5);
+        return cut_cross_b(ctp_of(pow(10.0, (double)-m)));
+    }
+    case RV_AI_AZS: {
+        const double tauA = fabs(b0 + b2 - 2 * b1);
+        return cut_cross_b(ctp_of(fmin(1e-5, tauA)));
+    }
+    case RV_AI_ASF1: case RV_AI_ASF2: case RV_AI_ASFAI1: {
+        const double x = fmin(1.0, eta_ai(kEpsA) / 0.24);
+        return cut_cross_b(0.157 / (11.351092 * x * x - 5.740650 * x + 1.506631));
+    }
+    case RV_ZYC: {
+        const double mn = fmin(1.0, 4.1666667 * eta_ai(2.7551 * 1e-7));
+        return cut_cong(0.157 / (11.351092 * mn * mn - 5.740650 * mn + 1.506631));
+    }
+    case RV_F203: case RV_F202: {
+        const double epsA = 2.7551 * 1e-7;
+        const double d0 = q0 - q1, d1 = q1 - q2, d2 = q2 - q3, d3 = q3 - q4;
+        const double e0 = (fabs(2.0 * d1 * d0) + epsA) / (d1 * d1 + d0 * d0 + epsA);
+        const double e1 = (fabs(2.0 * d2 * d1) + epsA) / (d2 * d2 + d1 * d1 + epsA);
+        const double e2 = (fabs(2.0 * d3 * d2) + epsA) / (d3 * d3 + d2 * d2 + epsA);
+        double emin = e0;
+        if (e1 < emin) emin = e1;
+        if (e2 < emin) emin = e2;
+        const double m = 1 - fmin(0.24, emin) / 0.24;
+        double CT;
+        if (variant == RV_F203) {
+            const double mm = m * m, mmm = m * mm;
+            CT = -0.452662 * mmm + 0.590811 * mm - 0.012189 * m + 0.022010;
+        } else {
+            CT = -0.088182 * m * m + 0.259395 * m - 0.000616;
+        }
+        return cut_cong(CT);
+    }
+    case RV_CONGAA: {
+        const double m = 1.0 - fmin(1.0, eta_raw() / 0.24);
+        const double g = pow(1 - m, 4.0) * (1 + 4 * m);
+        return cut_cong(pow(10.0, -round(10.0 - 5.0 * (1 - g))));
+    }
+    default:
+        return 7u;
+    }
 }
 
 template <int FAM>
@@ -245,6 +476,9 @@ CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, doub
         if (ll < rr * b1) flag += 2;
         if (ll < rr * b2) flag += 4;
         return teno_select(flag, q0, q1, q2, q3, q4);
+    } else if constexpr (FAM == FAM_RESEARCH) {
+        (void)kap;
+        return teno_select(research_flag((int)c, q0, q1, q2, q3, q4), q0, q1, q2, q3, q4);
     } else {
         // musclIn5: minmod limited slope on (q1, q2, q3).
         double deltam = q2 - q1, deltap = q3 - q2, delta;

@@ -245,7 +245,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             const double *spl = sp + l * LSP, *scl = sc + l * LSP;
             auto csacc = [&](int m, int v) { return scl[v * W * LSP + slot[m]]; };
             auto pracc = [&](int m, int v) { return spl[v * W * LSP + slot[m]]; };
-            if constexpr (PREC == 1) {
+            if constexpr (PREC == 1 && FAM != FAM_RESEARCH) {
                 const float2 *hll = shl + l * LSP;
                 // the FP32 hi/lo split of each stencil cell's cons
                 auto hlacc = [&](int m, int v) {
@@ -508,7 +508,7 @@ static cudaError_t launch_batched_shape(const BatchSweep &b, cudaStream_t st)
 {
     if (b.prec == 0) return launch_batched_shape_p<NV, AX, FAM, FLUX, S, W, 0>(b, st);
 #if defined(CFD_FAST)
-    if constexpr (NV >= 4) return launch_batched_shape_p<NV, AX, FAM, FLUX, S, W, 1>(b, st);
+    if constexpr (NV >= 4 && FAM != FAM_RESEARCH) return launch_batched_shape_p<NV, AX, FAM, FLUX, S, W, 1>(b, st);
 #endif
     return cudaErrorInvalidValue;
 }
@@ -519,7 +519,7 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
 {
     if (p.prec == 0) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 0>(p, st);
 #if defined(CFD_FAST)
-    if constexpr (NV >= 4) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 1>(p, st);
+    if constexpr (NV >= 4 && FAM != FAM_RESEARCH) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 1>(p, st);
 #endif
     return cudaErrorInvalidValue;
 }

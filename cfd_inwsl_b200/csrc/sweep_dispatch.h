@@ -17,7 +17,7 @@ template <int NV, int FAM>
 cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStream_t st);
 }
 
-#define CFD_FOR_EACH_FAMILY(X) X(0) X(1) X(2) X(3) X(4)
+#define CFD_FOR_EACH_FAMILY(X) X(0) X(1) X(2) X(3) X(4) X(5)
 
 #define CFD_DECL_EXTERN(NS, NV, F) \
     namespace NS { extern template cudaError_t launch_sweep<NV, F>(int, int, const SweepParams &, cudaStream_t); }

@@ -227,6 +227,27 @@ double ref_inter5(int inter_method, const double *q5)
     case congTCNS5CT5: return congTcns5_ZCT5(q);
     case congTCNS5CT10: return congTcns5_ZCT10(q);
     case MUCSLIN5: return musclIn5(q);
+    // the research variants (solverType.cpp:262-388 / 445-576)
+    case whfTCNSN: return whf_TcnsN(q);
+    case whfTCNSNA: return whf_TcnsN_A(q);
+    case whfTCNSNAS: return whf_TcnsN_AS(q);
+    case whfTCNSNS: return whf_TcnsN_S(q);
+    case whfTCNSNLAD: return whf_TcnsN_LAD(q);
+    case whfAITCNSNS: return whf_ai_TcnsN_S_1(q);
+    case whfAITCNSNA: return whf_ai_TcnsN_A_2(q);
+    case whfAITCNSNAS_1: return whf_ai_TcnsN_AS_1(q);
+    case whfAITCNSNAS_2: return whf_ai_TcnsN_AS_2(q);
+    case whfAITCNSNLADS: return whf_ai_TcnsN_LADS_yuanbao(q);
+    case whfAITCNSNAZS: return whf_ai_TcnsN_AZS_yuanbao(q);
+    case whfAITCNSNmyASF002_1: return whf_ai_TcnsN_myASF002_1(q);
+    case whfAITCNSNmyASF002_2: return whf_ai_TcnsN_myASF002_2(q);
+    case whfAITCNSNmyASF002_ai1: return whf_ai_TcnsN_myASF002_ai1(q);
+    case whfzycTCNSNmyASF002_1: return whf_zyc_TcnsN_myASF002_1(q);
+    case whfCOMPARE: return whf_TcnsN_COMPARE(q);
+    case new_WHFTCNSA: return new_whf_TCNS_A(q);
+    case new_WHFTCNSASF203_NoS: return whf_TCNS_AS_myF203_NoS(q);
+    case new_WHFTCNSASF202_NoS: return whf_TCNS_AS_myF202_NoS(q);
+    case 1010: return Teno5_CongAA(q);  // WCNS5CONGZCT7 as the 1D selector maps it
     default: return NAN;
     }
 }
