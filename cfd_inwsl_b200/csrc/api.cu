@@ -258,6 +258,7 @@ struct cfd_handle {
     long long ncell = 0;
     long long stride[3] = {1, 1, 1};
     int fam = 0;
+    int ng = 4;                  // ghost cells per line end (Info::nGhostCell)
     double icst = 0.0;
     double icst_k = 0.0;
     bool strict = false;
@@ -467,6 +468,7 @@ SweepParams base_params(cfd_handle *h, int d)
     p.halo_lo = h->halo[0];
     p.halo_hi = h->halo[1];
     p.halo_nl = h->ncell / h->cfg.n[h->dim - 1];
+    p.diff = h->cfg.diff_method;
     return p;
 }
 
@@ -653,9 +655,11 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     if (!cfg || !out) return CFD_ERR_CONFIG;
     *out = nullptr;
     if (cfg->dim < 1 || cfg->dim > 3) return CFD_ERR_CONFIG;
-    if (cfg->n_ghost != kGhost) return CFD_ERR_UNSUPPORTED;
+    if (cfg->diff_method != CFD_DIFF_MND6 && cfg->diff_method != CFD_DIFF_TRAD6) return CFD_ERR_UNSUPPORTED;
+    // Info::nGhostCell (info.cpp:7-22): WCNS5 + MND6 -> 4, WCNS5 + TRAD6 -> 5
+    if (cfg->n_ghost != (cfg->diff_method == CFD_DIFF_TRAD6 ? kGhost + 1 : kGhost)) return CFD_ERR_UNSUPPORTED;
     if (cfg->gamma != 1.4) return CFD_ERR_UNSUPPORTED;
-    if (cfg->diff_method != CFD_DIFF_MND6) return CFD_ERR_UNSUPPORTED;
+    if (cfg->diff_method == CFD_DIFF_TRAD6 && cfg->precision != CFD_PREC_FP64) return CFD_ERR_UNSUPPORTED;
     if (cfg->flux_method != CFD_FLUX_HLLC && cfg->flux_method != CFD_FLUX_ROE) return CFD_ERR_CONFIG;
     if (cfg->precision != CFD_PREC_FP64 && cfg->precision != CFD_PREC_MIXED) return CFD_ERR_CONFIG;
     // the mixed form reconstructs in FP32 (multi-dimensional fast flavour only);
@@ -680,6 +684,7 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     h->stride[1] = cfg->n[0];
     h->stride[2] = (long long)cfg->n[0] * cfg->n[1];
     h->fam = im.fam;
+    h->ng = cfg->n_ghost;
     h->icst = im.c;
     h->icst_k = (im.fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(im.c) : 0.0;
     h->strict = cfg->strict != 0;
@@ -764,16 +769,17 @@ int cfd_set_line_bc(cfd_handle *h, int idim, int i, int j, int side, int bnd_typ
     int t0, t1;
     transverse_axes(d, t0, t1);
     if (i < 0 || i >= h->cfg.n[t0] || j < 0 || j >= h->cfg.n[t1]) return fail(h, CFD_ERR_CONFIG, "line index out of range");
+    if (bnd_type == CFD_BND_HALO) return fail(h, CFD_ERR_CONFIG, "halo ends are wired by cfd_enable_halo");
     if (bnd_type != CFD_BND_PERIODIC_WRAP && (i0 < 0 || i0 >= h->ncell)) return fail(h, CFD_ERR_CONFIG, "i0 out of range");
     if (bnd_type == CFD_BND_PERIODIC1D || (bnd_type >= CFD_BND_SYMMETRYX && bnd_type <= CFD_BND_SYMMETRYZ) ||
         bnd_type == CFD_BND_SYMMETRY1D) {
-        long long last = i0 + (long long)(kGhost - 1) * offset;
+        long long last = i0 + (long long)(h->ng - 1) * offset;
         if (last < 0 || last >= h->ncell) return fail(h, CFD_ERR_CONFIG, "ghost source outside the grid");
     }
     int slot = -1;
     if (ghost_prim) {
-        slot = (int)(h->bc_vals.size() / (kGhost * h->nv));
-        h->bc_vals.insert(h->bc_vals.end(), ghost_prim, ghost_prim + kGhost * h->nv);
+        slot = (int)(h->bc_vals.size() / (h->ng * h->nv));
+        h->bc_vals.insert(h->bc_vals.end(), ghost_prim, ghost_prim + h->ng * h->nv);
     }
     long long lid = i + (long long)h->cfg.n[t0] * j;
     set_line(h, d, lid, side, bnd_type, i0, offset, slot);
@@ -1269,6 +1275,8 @@ int cfd_batch_create(const cfd_config *cfgs, int ncases, cfd_batch **out)
             a.strict != z.strict || a.precision != z.precision || a.device != z.device)
             return CFD_ERR_CONFIG;  // one kernel instantiation serves the batch
     }
+    for (int c = 0; c < ncases; c++)
+        if (cfgs[c].diff_method != CFD_DIFF_MND6) return CFD_ERR_UNSUPPORTED;  // the batched kernel is MND6 only
     cfd_batch *b = new cfd_batch();
     b->ncases = ncases;
     for (int c = 0; c < ncases; c++) {
@@ -1463,8 +1471,8 @@ namespace {
 int adjoint_supported(cfd_handle *h)
 {
     if (h->dim != 2 || h->fam != cfd::FAM_WCNS5 || h->cfg.flux_method != CFD_FLUX_ROE ||
-        h->cfg.precision != CFD_PREC_FP64 || h->cfg.source_type != 0)
-        return fail(h, CFD_ERR_UNSUPPORTED, "the adjoint covers 2D WCNS5 + Roe, FP64, without source terms");
+        h->cfg.precision != CFD_PREC_FP64 || h->cfg.source_type != 0 || h->cfg.diff_method != CFD_DIFF_MND6)
+        return fail(h, CFD_ERR_UNSUPPORTED, "the adjoint covers 2D WCNS5 + Roe + MND6, FP64, without source terms");
     for (int d = 0; d < 2; d++)
         for (int sd = 0; sd < 2; sd++)
             if (h->cfg.bc[d][sd] != CFD_BND_PERIODIC_WRAP)
@@ -1557,7 +1565,8 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
     int rc;
     if ((rc = adjoint_supported(h)) || (rc = sync_bc(h))) return rc;
     const size_t nck = (size_t)((nsteps + ckpt_every - 1) / ckpt_every);
-    adjoint_release(h->adj_ckpt);
+    // checkpoint buffers persist across records (they only grow): no
+    // cudaFree / cudaMalloc pair on the timed path of repeated gradients
     if ((rc = adjoint_states(h, h->adj_ckpt, nck))) return rc;
     const size_t state = sizeof(double) * h->ncell * h->nv;
     CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
@@ -1632,6 +1641,7 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
 int cfd_enable_halo(cfd_handle *h, int side, double **buf, long long *count)
 {
     if (!h || !buf || !count || (side != 0 && side != 1) || h->dim < 2) return CFD_ERR_CONFIG;
+    if (h->ng != kGhost) return fail(h, CFD_ERR_UNSUPPORTED, "slab halos carry 4 rows (MND6 only)");
     const int d = h->dim - 1;
     const long long nl = nlines(h, d);
     const long long n = (long long)h->nv * 4 * nl;

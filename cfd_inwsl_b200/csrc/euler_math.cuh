@@ -1406,4 +1406,20 @@ CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fh
 #endif
 }
 
+// ExplicitDif6::solve (differ.cpp:23-52): the sixth-order explicit difference
+// of the face fluxes x_{i-5/2} .. x_{i+5/2} (no node fluxes), in the
+// reference's order of operations.
+CFD_HD double trad6(double fhm5, double fhm3, double fhm1, double fhp1, double fhp3, double fhp5, double h,
+                    double inv_h)
+{
+    const double w0 = 75.0 / 64.0, w1 = 25.0 / (128.0 * 3.0), w2 = 3.0 / (128.0 * 5.0);
+#if defined(CFD_FAST)
+    (void)h;
+    return (w0 * (fhp1 - fhm1) - w1 * (fhp3 - fhm3) + w2 * (fhp5 - fhm5)) * inv_h;
+#else
+    (void)inv_h;
+    return (w0 * (fhp1 - fhm1) - w1 * (fhp3 - fhm3) + w2 * (fhp5 - fhm5)) / h;
+#endif
+}
+
 } // namespace cfd

@@ -44,7 +44,7 @@ __device__ __forceinline__ void load_cons_prim(const double *__restrict__ u, lon
 
 // Ghost cell k (0 = nearest the boundary) of a line end, as OneDBnd::update
 // leaves it after Bnds::update (oneDBnd.cpp:31-114).
-template <int NV>
+template <int NV, int NG>
 __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &bl, int k, double tstage, double *pr)
 {
     switch (bl.type) {
@@ -63,7 +63,7 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
         if (neg < NV - 1) pr[neg] = -pr[neg];
         if (bl.type == BND_SYMMETRY1D) {
             // SYMMETRY1D writes only the first three values of each ghost cell.
-            for (int v = 3; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * 4 + k) * NV + v] : 0.0;
+            for (int v = 3; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * NG + k) * NV + v] : 0.0;
         }
         return;
     }
@@ -85,7 +85,8 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     case BND_HALO: {
         // rows of the neighbouring slab, ascending: the low side's nearest
         // ghost is the neighbour's last row, the high side's its first
-        const int r = (bl.offset == 0) ? 3 - k : k;
+        const int kk = k > 3 ? 3 : k;  // four halo rows (MND6 only)
+        const int r = (bl.offset == 0) ? 3 - kk : kk;
         const double *hb = (bl.offset == 0) ? p.halo_lo : p.halo_hi;
         double c[NV];
 #pragma unroll
@@ -95,7 +96,7 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     }
     default:
         // DIRICLET and every type whose update() is a no-op keep their static data.
-        for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * 4 + k) * NV + v] : 0.0;
+        for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * NG + k) * NV + v] : 0.0;
         return;
     }
 }
@@ -107,12 +108,17 @@ constexpr int pow2_ceil(int x)
     return r;
 }
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC = 0>
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC = 0, int DIFF = 0>
 struct SweepShape {
     static constexpr int NT = S * W;
+    // Halo cells per side: MND6 differences faces x_{i-3/2}..x_{i+3/2} (cells
+    // i-4..i+4), TRAD6 faces x_{i-5/2}..x_{i+5/2} (cells i-5..i+5). A chunk
+    // shares FC = 2 HG - 5 faces with the previous one.
+    static constexpr int HG = DIFF ? 5 : 4;
+    static constexpr int FC = 2 * HG - 5;
     // ring sizes are powers of two so that ring positions are bit masks
-    static constexpr int R = pow2_ceil(S + 8);   // prim ring positions (S + 8 used)
-    static constexpr int RF = pow2_ceil(S + 3);  // face ring positions (S + 3 used)
+    static constexpr int R = pow2_ceil(S + 2 * HG);  // prim ring positions (S + 2 HG used)
+    static constexpr int RF = pow2_ceil(S + FC);     // face ring positions (S + FC used)
     static constexpr int LSP = R | 1;         // odd line strides avoid bank conflicts
     static constexpr int LSF = RF | 1;
     static constexpr int SMEM_DOUBLES = 2 * NV * W * LSP + NV * W * LSF;
@@ -132,14 +138,15 @@ struct SweepShape {
     static constexpr size_t SMEM_BYTES = SMEM_RINGS + (PF ? SMEM_STAGE : 0);
 };
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
 #ifndef CFD_SWEEP_MINB
 #define CFD_SWEEP_MINB 2
 #endif
 __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 {
-    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC>;
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC, DIFF>;
     constexpr int NT = SH::NT, R = SH::R, RF = SH::RF, LSP = SH::LSP, LSF = SH::LSF;
+    constexpr int HG = SH::HG, FC = SH::FC, FO = HG - 3;  // face j sits at face-ring position j - s_begin + FO
     // device-resident loop: the whole launch is a no-op once the loop is done
     if (p.ctl && p.ctl->done) return;
     const double tstage = p.ctl ? p.ctl->tst[p.rk_stage] : p.t;
@@ -205,14 +212,14 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             }
         } else if (P < 0) {
             int k = -P - 1;
-            ghost_prim<NV>(p, p.bc_lo[lid], k > 3 ? 3 : k, tstage, pr);
+            ghost_prim<NV, HG>(p, p.bc_lo[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
         } else {
             int k = P - nd;
-            ghost_prim<NV>(p, p.bc_hi[lid], k > 3 ? 3 : k, tstage, pr);
+            ghost_prim<NV, HG>(p, p.bc_hi[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
         }
         double cs[NV];
         prim_to_cons<NV>(pr, cs);
-        int slot = ring(P - s_begin + 4);
+        int slot = ring(P - s_begin + HG);
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             sp[(v * W + l) * LSP + slot] = pr[v];
@@ -228,7 +235,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     auto face = [&](int l, int j) {
         int slot[6];
 #pragma unroll
-        for (int m = 0; m < 6; m++) slot[m] = ring(j - 3 + m - s_begin + 4);
+        for (int m = 0; m < 6; m++) slot[m] = ring(j - 3 + m - s_begin + HG);
         double fl[NV], fr[NV], fx[NV];
         if constexpr (NV == 3) {
             double pr6[6][NV], cs6[6][NV];
@@ -258,16 +265,16 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         }
         if constexpr (PREC == 1 && FLUX == FLUX_ROE && NV >= 4) roe_md_mixed<NV, AX>(fl, fr, fx);
         else riemann<NV, AX, FLUX>(fl, fr, fx);
-        int fslot = fring(j - s_begin + 1);
+        int fslot = fring(j - s_begin + FO);
 #pragma unroll
         for (int v = 0; v < NV; v++) sf[(v * W + l) * LSF + fslot] = fx[v];
     };
 
-    // prologue: cells s_begin-4 .. s_begin+3
-    for (int idx = tid; idx < 8 * W; idx += NT) {
-        int l = (AX == 0) ? idx / 8 : idx % W;
-        int q = (AX == 0) ? idx % 8 : idx / W;
-        load_pos(l, s_begin - 4 + q);
+    // prologue: cells s_begin-HG .. s_begin+HG-1
+    for (int idx = tid; idx < 2 * HG * W; idx += NT) {
+        int l = (AX == 0) ? idx / (2 * HG) : idx % W;
+        int q = (AX == 0) ? idx % (2 * HG) : idx / W;
+        load_pos(l, s_begin - HG + q);
     }
 
     double red_rho = 0.0, red_lam[3] = {0.0, 0.0, 0.0};
@@ -302,26 +309,26 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         }
         __pipeline_commit();
     };
-    if constexpr (PF) prefetch_cell(s_begin + 4 + tp);
+    if constexpr (PF) prefetch_cell(s_begin + HG + tp);
 
     for (int c0 = s_begin; c0 < s_end; c0 += S) {
         if constexpr (PF) {
             __pipeline_wait_prior(0);
-            load_pos(tl, c0 + 4 + tp, true);
+            load_pos(tl, c0 + HG + tp, true);
             prefetch_epilogue(c0 + tp);
-            prefetch_cell(c0 + S + 4 + tp);  // an empty group past the segment
+            prefetch_cell(c0 + S + HG + tp);  // an empty group past the segment
         } else {
-            load_pos(tl, c0 + 4 + tp);
+            load_pos(tl, c0 + HG + tp);
         }
         __syncthreads();
-        if (c0 == s_begin) {
-            for (int idx = tid; idx < 3 * W; idx += NT) {
-                int l = (AX == 0) ? idx / 3 : idx % W;
-                int q = (AX == 0) ? idx % 3 : idx / W;
-                face(l, s_begin - 1 + q);
+        if (c0 == s_begin) {  // the FC faces before the chunk's first new one
+            for (int idx = tid; idx < FC * W; idx += NT) {
+                int l = (AX == 0) ? idx / FC : idx % W;
+                int q = (AX == 0) ? idx % FC : idx / W;
+                face(l, s_begin - FO + q);
             }
         }
-        face(tl, c0 + 2 + tp);
+        face(tl, c0 + HG - 2 + tp);
         __syncthreads();
 
         const int i = c0 + tp;
@@ -329,23 +336,30 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         line_of(tl, ok, base, lid);
         if constexpr (PF) __pipeline_wait_prior(1);  // the epilogue operands; the next cell may still fly
         if (ok && i < s_end) {
-            double pm[NV], pp[NV], fnm[NV], fnp[NV];
-            int sm = ring(i - 1 - s_begin + 4), spp = ring(i + 1 - s_begin + 4);
+            double fnm[NV], fnp[NV];
+            if constexpr (DIFF == 0) {  // node fluxes of cells i-1 and i+1 (SolvePointSolver, nl = nr = 1)
+                double pm[NV], pp[NV];
+                int sm = ring(i - 1 - s_begin + HG), spp = ring(i + 1 - s_begin + HG);
 #pragma unroll
-            for (int v = 0; v < NV; v++) {
-                pm[v] = sp[(v * W + tl) * LSP + sm];
-                pp[v] = sp[(v * W + tl) * LSP + spp];
+                for (int v = 0; v < NV; v++) {
+                    pm[v] = sp[(v * W + tl) * LSP + sm];
+                    pp[v] = sp[(v * W + tl) * LSP + spp];
+                }
+                node_flux<NV, AX>(pm, fnm);
+                node_flux<NV, AX>(pp, fnp);
             }
-            node_flux<NV, AX>(pm, fnm);
-            node_flux<NV, AX>(pp, fnp);
-            int f0 = fring(i - 1 - s_begin + 1), f1 = fring(i - s_begin + 1), f2 = fring(i + 1 - s_begin + 1),
-                f3 = fring(i + 2 - s_begin + 1);
+            // faces j = i-(FC-1)/2 .. i+(FC+1)/2, face j being x_{j-1/2}
+            int fs[FC + 1];
+#pragma unroll
+            for (int m = 0; m <= FC; m++) fs[m] = fring(i - (FC - 1) / 2 + m - s_begin + FO);
             const long long cell = base + (long long)i * sAX;
             double uo[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 const double *fv = sf + (v * W + tl) * LSF;
-                double d = mnd6(fnm[v], fnp[v], fv[f0], fv[f1], fv[f2], fv[f3], p.h, inv_h);
+                double d;
+                if constexpr (DIFF == 0) d = mnd6(fnm[v], fnp[v], fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]], p.h, inv_h);
+                else d = trad6(fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]], fv[fs[4]], fv[fs[5]], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
                 const double *sv = stg + v * NT + tid;
                 double r = p.first ? (0.0 + d) : ((PF_EPI ? sv[1 * NV * NT] : p.rhs[gi]) + d);
@@ -353,7 +367,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                     // SourceTerm::calGravitySource (sourceTerm.cpp:3-20) on the
                     // stage's prim: rhs(rho v) -= rho, rhs(rho E) -= rho v
                     if (p.gravity) {
-                        const int sc0 = ring(i - s_begin + 4);
+                        const int sc0 = ring(i - s_begin + HG);
                         const double rho = sp[(0 * W + tl) * LSP + sc0];
                         if (v == 2) r -= rho;
                         if (v == 3) r -= rho * sp[(2 * W + tl) * LSP + sc0];
@@ -398,11 +412,11 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     }
 }
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
 __global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
     sweep_kernel(const __grid_constant__ SweepParams p)
 {
-    sweep_tile<NV, AX, FAM, FLUX, S, W, PREC>(p, blockIdx.x);
+    sweep_tile<NV, AX, FAM, FLUX, S, W, PREC, DIFF>(p, blockIdx.x);
 }
 
 // Number of CTA tiles one case's sweep along AX needs.
@@ -446,15 +460,15 @@ __global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
             for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
         }
         __syncthreads();
-        sweep_tile<NV, AX, FAM, FLUX, S, W, PREC>(sp, (int)(item - tile_start[c]));
+        sweep_tile<NV, AX, FAM, FLUX, S, W, PREC, 0>(sp, (int)(item - tile_start[c]));
     }
 }
 
-template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
+template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
 static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
 {
-    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC>;
-    auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC>;
+    using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC, DIFF>;
+    auto kern = sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC, DIFF>;
     // the dynamic shared-memory opt-in is per device
     static bool attr_set[64] = {};
     int dev = 0;
@@ -472,7 +486,7 @@ static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
     long long nblk = (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
     if (nblk <= 0) return cudaSuccess;
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
+    sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC, DIFF><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
     return cudaGetLastError();
 }
 
@@ -513,13 +527,16 @@ static cudaError_t launch_batched_shape(const BatchSweep &b, cudaStream_t st)
     return cudaErrorInvalidValue;
 }
 
-// FP64 or, in the fast flavour of the multi-dimensional kernels, mixed.
+// FP64 or, in the fast flavour of the multi-dimensional kernels, mixed; the
+// TRAD6 difference in FP64 only.
 template <int NV, int AX, int FAM, int FLUX, int S, int W>
 static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
 {
-    if (p.prec == 0) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 0>(p, st);
+    if (p.diff == DIFF_TRAD6) return p.prec == 0 ? launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 0, 1>(p, st)
+                                                 : cudaErrorInvalidValue;
+    if (p.prec == 0) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 0, 0>(p, st);
 #if defined(CFD_FAST)
-    if constexpr (NV >= 4 && FAM != FAM_RESEARCH) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 1>(p, st);
+    if constexpr (NV >= 4 && FAM != FAM_RESEARCH) return launch_sweep_shape_p<NV, AX, FAM, FLUX, S, W, 1, 0>(p, st);
 #endif
     return cudaErrorInvalidValue;
 }

@@ -50,6 +50,10 @@ struct BcLine {
     double dh_y;   // DoubleMachUp: edge cell centre minus its inner neighbour, y
 };
 
+// DiffMethod values (zone_FD/src/include/macro.hpp:82) the sweeps implement;
+// any other value of SweepParams::diff runs MND6.
+enum : int { DIFF_TRAD6 = 1, DIFF_MND6 = 3 };
+
 enum SweepMode : int { MODE_WRITE = 0, MODE_RK = 2 };
 enum ErrBits : unsigned { ERR_NONFINITE = 1u, ERR_NEGATIVE = 2u, ERR_TIMEOUT = 4u };
 
@@ -82,7 +86,7 @@ struct SweepParams {
     unsigned *err;      // ErrBits
     const BcLine *bc_lo;  // per line (index a + n[T0] * b), low end
     const BcLine *bc_hi;  // per line, high end
-    const double *bc_vals; // static ghost prim values [slot][4][NV]
+    const double *bc_vals; // static ghost prim values [slot][ghosts per side][NV]
     double t;           // stage time (ignored when ctl is set)
     const StepCtl *ctl; // device-resident step control (null: use rkBdt/t)
     double dm_u, dm_v;  // DoubleMachUp post-shock velocity, 8.25 cos(pi/6) and -8.25 sin(pi/6) from the host libm
@@ -93,6 +97,8 @@ struct SweepParams {
     int gravity;        // 1: add the gravity source of the stage's input state (last direction only)
     const double *halo_lo, *halo_hi;  // BND_HALO ghosts: [var][4 rows, ascending][line]
     long long halo_nl;                // lines per halo row
+    int diff;                         // DIFF_TRAD6: ExplicitDif6 with 5 ghosts; else MND6 with 4
+    int pad_diff;
 };
 
 // One batched sweep launch: the parameter blocks of every case (device array)

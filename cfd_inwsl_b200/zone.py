@@ -159,8 +159,8 @@ class Info:
 
     nCons = nPrim
 
-    def nGhostCell(self) -> int:  # info.cpp:7-22 (WCNS5 + MND6)
-        return 4
+    def nGhostCell(self) -> int:  # info.cpp:7-22 (spMethod WCNS5)
+        return {DiffMethod.MND6: 4, DiffMethod.TRAD6: 5, DiffMethod.HDS6: 3}.get(DiffMethod(self.diffMethod), 0)
 
 
 def default_bc_types(info: Info) -> list[list[int]]:
@@ -199,6 +199,7 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
     cfg.inter_method = int(info.interMethod)
     cfg.flux_method = int(info.fluxMethod)
     cfg.diff_method = int(info.diffMethod)
+    cfg.n_ghost = info.nGhostCell()
     cfg.strict = int(bool(info.strict))
     cfg.precision = int(getattr(info, "precision", 0))
     cfg.device = int(info.device)
@@ -212,10 +213,10 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
     return cfg
 
 
-def _set_line_bc(lib, h, nvar, idim, i, j, side, bnd_type, i0=0, offset=0, ghost_prim=None):
+def _set_line_bc(lib, h, nvar, idim, i, j, side, bnd_type, i0=0, offset=0, ghost_prim=None, nghost=4):
     gp = None
     if ghost_prim is not None:
-        gp = np.ascontiguousarray(np.broadcast_to(np.asarray(ghost_prim, dtype=np.float64), (4, nvar)))
+        gp = np.ascontiguousarray(np.broadcast_to(np.asarray(ghost_prim, dtype=np.float64), (nghost, nvar)))
     _lib.check(lib.cfd_set_line_bc(h, idim, i, j, side, int(bnd_type), int(i0), int(offset),
                                    _lib.ptr(gp) if gp is not None else None), h)
 
@@ -230,23 +231,25 @@ def wire_case_bnds(lib, h, info: Info):
     n = info.icMax()
     nx, ny = n[0], n[1]
     nv = info.nPrim()
+    ng = info.nGhostCell()
     if info.nCase == 3:
         for i in range(nx):
-            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, [2.0, 0, 0, 1.0])
-            _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DIRICLET, i + (ny - 1) * nx, -nx, [1.0, 0, 0, 2.5])
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, [2.0, 0, 0, 1.0], nghost=ng)
+            _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DIRICLET, i + (ny - 1) * nx, -nx, [1.0, 0, 0, 2.5],
+                         nghost=ng)
         return
     post = [8.0, 8.25 * math.cos(math.pi / 6), -8.25 * math.sin(math.pi / 6), 116.5]
     hx = info.geth(0)
     for j in range(ny):
-        _set_line_bc(lib, h, nv, 1, j, 0, 0, BndType.DIRICLET, j * nx, 1, post)
-        _set_line_bc(lib, h, nv, 1, j, 0, 1, BndType.SUPERSONICOUTLET, j * nx + nx - 1, -1)
+        _set_line_bc(lib, h, nv, 1, j, 0, 0, BndType.DIRICLET, j * nx, 1, post, nghost=ng)
+        _set_line_bc(lib, h, nv, 1, j, 0, 1, BndType.SUPERSONICOUTLET, j * nx + nx - 1, -1, nghost=ng)
     for i in range(nx):
         x = info.calZone[0] + (i + 0.5) * hx  # Block::coorCel as initializer.cpp:677 fills it
         if x < 1.0 / 6.0:
-            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, post)
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.DIRICLET, i, nx, post, nghost=ng)
         else:
-            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.SYMMETRYY, i, nx)
-        _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DoubleMachUp, i + (ny - 1) * nx, -nx)
+            _set_line_bc(lib, h, nv, 2, i, 0, 0, BndType.SYMMETRYY, i, nx, nghost=ng)
+        _set_line_bc(lib, h, nv, 2, i, 0, 1, BndType.DoubleMachUp, i + (ny - 1) * nx, -nx, nghost=ng)
 
 
 class BlockSolver:
@@ -290,7 +293,8 @@ class BlockSolver:
     def set_line_bc(self, idim: int, i: int, j: int, side: int, bnd_type: int, i0: int = 0, offset: int = 0,
                     ghost_prim=None):
         """Mirror of OneDBnd::setUpdate/setValue for one line end (idim 1-based)."""
-        _set_line_bc(self.lib, self.h, self.nvar, idim, i, j, side, bnd_type, i0, offset, ghost_prim)
+        _set_line_bc(self.lib, self.h, self.nvar, idim, i, j, side, bnd_type, i0, offset, ghost_prim,
+                     self.info.nGhostCell())
 
     # --- state access (reference AoS layout)
     def set_cons(self, cons: np.ndarray):
@@ -451,7 +455,7 @@ class BlockBatch:
                     offset: int = 0, ghost_prim=None):
         """BlockSolver.set_line_bc on one case of the batch."""
         _set_line_bc(self.lib, self.cases[case], self._shape(case)[1], idim, i, j, side, bnd_type, i0, offset,
-                     ghost_prim)
+                     ghost_prim, self.infos[case].nGhostCell())
 
     def set_cons(self, i, cons):
         nc, nv = self._shape(i)

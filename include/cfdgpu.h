@@ -48,7 +48,11 @@ extern "C" {
 #define CFD_FLUX_HLLC 0
 #define CFD_FLUX_ROE 1
 
-/* DiffMethod (macro.hpp:82); only MND6 is implemented. */
+/* DiffMethod (macro.hpp:82). MND6 (MidNodeAndNodeDif6, 4 ghosts) and TRAD6
+ * (ExplicitDif6, differ.cpp:23-52, 5 ghosts) are implemented; HDS6 has no
+ * differ in the reference (SolverType::initDiffer, solverType.cpp:657-681) and
+ * TRAD2 no ghost count with a five-point interpolation (info.cpp:7-22). */
+#define CFD_DIFF_TRAD6 1
 #define CFD_DIFF_MND6 3
 
 /* Arithmetic of the sweep kernels. */
@@ -75,11 +79,12 @@ typedef struct cfd_config {
     int n[3];           /* cells per direction (Info::icMax()); 1 for unused directions */
     double h[3];        /* spacing per direction; the reference uses one h for all (Info::geth) */
     double x0[3];       /* lower corner of the domain (Info::calZone[0,2,4]) */
-    int n_ghost;        /* must be 4 (Info::nGhostCell for WCNS5 + MND6, info.cpp:11) */
+    int n_ghost;        /* Info::nGhostCell (info.cpp:7-22): 4 with MND6, 5 with TRAD6 */
     double gamma;       /* must be 1.4 (macro.hpp:28 GAMMA) */
     int inter_method;   /* InterMethod enum value (macro.hpp:37-78) */
     int flux_method;    /* CFD_FLUX_HLLC or CFD_FLUX_ROE */
-    int diff_method;    /* CFD_DIFF_MND6 */
+    int diff_method;    /* CFD_DIFF_MND6 or CFD_DIFF_TRAD6 (TRAD6: FP64 only; not in batches,
+                           slabs, the adjoint or cfd_rhs_noalloc) */
     int precision;      /* CFD_PREC_FP64 or CFD_PREC_MIXED */
     int strict;         /* 1: reference operation order, no FMA contraction (bitwise parity build) */
     int bc[3][2];       /* default boundary type per direction and side (0 = low, 1 = high),

@@ -10,6 +10,7 @@
  *   Riemann fluxes      zone_FD/src/include/fluxSchemes.hpp:13-71, 74-125, 202-327, 420-553
  *   node fluxes         fluxSchemes.hpp:572-599, solvePointFlux.hpp:33-100
  *   MND6                zone_FD/src/src/differ.cpp:54-103
+ *   TRAD6               zone_FD/src/src/differ.cpp:23-52 (ghosts: info.cpp:7-22)
  *   cons -> prim        zone_FD/src/src/equation.cpp:37-93
  *   boundaries          zone_FD/src/src/oneDBnd.cpp:31-114
  *   RK3 and CFL step    zone_FD/src/src/blockSolver.cpp:43-87, 318-349
@@ -503,16 +504,28 @@ static void sweep_line(const orc_cfg *c, const double *prim, double *rhs, int d,
                        double (*Fh)[MAXV], double (*Fn)[MAXV])
 {
     int nv = nvar_of(c->dim), n = c->n[d];
+    int ng = c->diff ? 5 : 4, nf = n + 2 * ng - 5;
     long long s = strides(c, d);
-    /* P[0..n+7] = ghosts 3..0 (reversed, reconstructor5order.hpp:144-164), cells, ghosts 0..3 */
-    for (int k = 0; k < 4; k++) ghost(c, prim, d, 0, first, k, P[3 - k]);
-    for (int i = 0; i < n; i++) memcpy(P[4 + i], prim + (first + i * s) * nv, sizeof(double) * nv);
-    for (int k = 0; k < 4; k++) ghost(c, prim, d, 1, first, k, P[4 + n + k]);
-    /* n+3 faces x_{-3/2} .. x_{n+1/2}: face f uses P[f .. f+5] */
-    for (int f = 0; f < n + 3; f++) {
+    /* P[0..n+2ng-1] = ghosts ng-1..0 (reversed, reconstructor5order.hpp:64-84), cells, ghosts 0..ng-1 */
+    for (int k = 0; k < ng; k++) ghost(c, prim, d, 0, first, k, P[ng - 1 - k]);
+    for (int i = 0; i < n; i++) memcpy(P[ng + i], prim + (first + i * s) * nv, sizeof(double) * nv);
+    for (int k = 0; k < ng; k++) ghost(c, prim, d, 1, first, k, P[ng + n + k]);
+    /* nf faces x_{-(2ng-5)/2} .. x_{n-1+(2ng-5)/2}: face f uses P[f .. f+5] */
+    for (int f = 0; f < nf; f++) {
         double fl[MAXV], fr[MAXV];
         recon_face(c, d, P + f, fl, fr);
         riemann(c, d, fl, fr, Fh[f]);
+    }
+    if (c->diff) {
+        /* ExplicitDif6: faces Fh[i] .. Fh[i+5] are x_{i-5/2} .. x_{i+5/2} */
+        const double w0 = 75.0 / 64.0, w1 = 25.0 / (128.0 * 3.0), w2 = 3.0 / (128.0 * 5.0);
+        for (int i = 0; i < n; i++) {
+            double *r = rhs + (first + i * s) * nv;
+            for (int v = 0; v < nv; v++)
+                r[v] += (w0 * (Fh[i + 3][v] - Fh[i + 2][v]) - w1 * (Fh[i + 4][v] - Fh[i + 1][v]) +
+                         w2 * (Fh[i + 5][v] - Fh[i][v])) / c->h;
+        }
+        return;
     }
     /* n+2 nodes x_{-1} .. x_n (ghost 0 on each side, nl = nr = 1) */
     for (int m = 0; m < n + 2; m++) phys_flux(nv, d, P[3 + m], Fn[m]);
@@ -536,8 +549,8 @@ void orc_rhs(const orc_cfg *c, const double *cons, double *rhs)
         long long nl = nc / n;
 #pragma omp parallel num_threads(c->threads > 0 ? c->threads : omp_get_max_threads())
         {
-            double (*P)[MAXV] = malloc(sizeof(double) * MAXV * (n + 8));
-            double (*Fh)[MAXV] = malloc(sizeof(double) * MAXV * (n + 3));
+            double (*P)[MAXV] = malloc(sizeof(double) * MAXV * (n + 10));
+            double (*Fh)[MAXV] = malloc(sizeof(double) * MAXV * (n + 5));
             double (*Fn)[MAXV] = malloc(sizeof(double) * MAXV * (n + 2));
 #pragma omp for schedule(static)
             for (long long l = 0; l < nl; l++) {

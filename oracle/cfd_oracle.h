@@ -31,6 +31,7 @@ typedef struct orc_cfg {
     int bc[3][2];     /* ORC_OUTLET / ORC_SYMMETRY (normal velocity negated) / ORC_WRAP /
                          ORC_MIRRORCOPY (PERIODIC1D with the reference's default wiring) */
     int threads;      /* OpenMP threads (0 = runtime default) */
+    int diff;         /* 0: MND6 (4 ghosts), 1: TRAD6 (ExplicitDif6, 5 ghosts) */
 } orc_cfg;
 
 /* rhs (AoS, ncell*nvar) of cons (AoS) */

@@ -65,6 +65,7 @@ struct ref_cfg {
     int n_case;         // Info::nCase: selects the initial state and BC wiring
     double cfl;         // Info::CFL
     int source_type;    // Info::sourceType (0 SOURCENULL, 1 GRAVITY)
+    int diff_method;    // Info::diffMethod (DiffMethod: HDS6 0, TRAD6 1, TRAD2 2, MND6 3)
 };
 
 struct ref_handle {
@@ -77,7 +78,7 @@ void *ref_create(const ref_cfg *c)
     Info *info = new Info();
     info->eqType = EULER;
     info->spMethod = WCNS5;
-    info->diffMethod = MND6;
+    info->diffMethod = (DiffMethod)c->diff_method;
     info->fluxMethod = (FluxMethod)c->flux_method;
     info->interMethod = (InterMethod)c->inter_method;
     info->nCase = c->n_case;

@@ -19,7 +19,8 @@ REF_LIB = HERE / "_ref" / "libcongfd_ref.so"
 
 class RefCfg(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("zone", C.c_double * 6), ("inter_method", C.c_int),
-                ("flux_method", C.c_int), ("n_case", C.c_int), ("cfl", C.c_double), ("source_type", C.c_int)]
+                ("flux_method", C.c_int), ("n_case", C.c_int), ("cfl", C.c_double), ("source_type", C.c_int),
+                ("diff_method", C.c_int)]
 
 
 _lib = None
@@ -82,14 +83,15 @@ class RefSolver:
     """
 
     def __init__(self, dim, n, zone, inter_method=2, flux_method=0, n_case=0, cfl=0.5, periodic=False, threads=None,
-                 source_type=0):
+                 source_type=0, diff_method=3):
         self.lib = load()
         if threads is not None:
             self.lib.ref_set_threads(int(threads))
         n3 = list(n) + [1] * (3 - len(n))
         cfg = RefCfg(dim, (C.c_int * 3)(*n3), (C.c_double * 6)(*zone), inter_method, flux_method, n_case, cfl,
-                     source_type)
+                     source_type, diff_method)
         self.h = self.lib.ref_create(C.byref(cfg))
+        self.ng = 5 if diff_method == 1 else 4  # Info::nGhostCell (info.cpp:7-22)
         self.dim = dim
         self.n = n3
         self.ncell = self.lib.ref_ncells(self.h)
@@ -122,7 +124,7 @@ class RefSolver:
             self.lib.ref_set_line_bc(self.h, 2, i, 0, 1, 1, i, nx, None)
 
     def set_line_bc(self, idim, i, j, side, typ, i0, offset, values=None):
-        v = None if values is None else np.ascontiguousarray(np.broadcast_to(np.asarray(values, float), (4, self.nvar)))
+        v = None if values is None else np.ascontiguousarray(np.broadcast_to(np.asarray(values, float), (self.ng, self.nvar)))
         rc = self.lib.ref_set_line_bc(self.h, idim, i, j, side, int(typ), int(i0), int(offset),
                                       _p(v) if v is not None else None)
         assert rc == 0
@@ -217,7 +219,7 @@ ORC_FAMILY = {2: (0, 0.0), 3: (1, 0.0), 11: (2, 1e-5), 12: (2, 1e-4), 13: (2, 1e
 
 class OrcCfg(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("h", C.c_double), ("fam", C.c_int), ("icst", C.c_double),
-                ("flux", C.c_int), ("bc", (C.c_int * 2) * 3), ("threads", C.c_int)]
+                ("flux", C.c_int), ("bc", (C.c_int * 2) * 3), ("threads", C.c_int), ("diff", C.c_int)]
 
 
 _orc = None
@@ -245,13 +247,13 @@ def orc_load() -> C.CDLL:
 class OracleC:
     """The plain-C restatement (1D/2D/3D) on a uniform grid with per-side BC kinds."""
 
-    def __init__(self, dim, n, h, inter_method=2, flux_method=0, bc=None, threads=0):
+    def __init__(self, dim, n, h, inter_method=2, flux_method=0, bc=None, threads=0, trad6=False):
         self.lib = orc_load()
         fam, icst = ORC_FAMILY[inter_method]
         n3 = list(n) + [1] * (3 - len(n))
         bcs = bc if bc is not None else [[ORC_OUTLET] * 2] * 3
         arr = ((C.c_int * 2) * 3)(*[(C.c_int * 2)(*bcs[d]) for d in range(3)])
-        self.cfg = OrcCfg(dim, (C.c_int * 3)(*n3), h, fam, icst, flux_method, arr, threads)
+        self.cfg = OrcCfg(dim, (C.c_int * 3)(*n3), h, fam, icst, flux_method, arr, threads, int(bool(trad6)))
         self.nvar = dim + 2
         self.ncell = n3[0] * n3[1] * n3[2]
         self.cons = None

@@ -19,6 +19,10 @@ file the reference repository commits:
   sod_400.npz                1D Sod, 400 cells, WCNS5 + HLLC, CFL 0.5, t = 0.2
   kat_face.npz               one-face characteristic reconstructions (reconI,
                              reconstructor5order.hpp:233-429), 1D and 2D, both normals
+  rhs_trad6.npz              one RHS, one CFL step and one RK3 step with the TRAD6
+                             difference (Info::diffMethod = TRAD6, 5 ghosts), 1D and 2D
+
+    python tests/golden/make_golden.py rhs_trad6   (one fixture only)
 """
 from __future__ import annotations
 
@@ -181,7 +185,48 @@ def kat_face(rng):
     return out
 
 
+def line_state(n, rng):
+    """Three constant 1D regions (random prim) on n cells."""
+    P = np.array([[rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(0.05, 2)] for _ in range(3)])
+    q = np.minimum((np.arange(n) * 3) // n, 2)
+    return prim_to_cons(P[q])
+
+
+def rhs_trad6(rng):
+    """TRAD6 (ExplicitDif6, differ.cpp:23-52) through the reference's own solver."""
+    out = {}
+    cases = [(1, "line", 40, 2, 0, 0, False), (1, "line", 40, 11, 1, 0, False), (1, "line", 40, 8, 0, 4, False),
+             (1, "line", 40, 3, 1, 0, True), (2, "quad", 16, 2, 0, 0, False), (2, "quad", 16, 11, 1, 2, False),
+             (2, "quad", 16, 8, 0, 6, False), (2, "smooth", 16, 35, 1, 0, True), (2, "quad", 16, 15, 1, 0, False),
+             (2, "smooth", 16, 3, 0, 0, True)]
+    meta = []
+    for k, (dim, kind, n, im, fm, ncase, periodic) in enumerate(cases):
+        if kind == "line":
+            cons = line_state(n, rng)
+            shape, zone = [n], [0, 1, 0, 0, 0, 0]
+        else:
+            cons = quadrant_state(n, rng) if kind == "quad" else smooth_state(n, rng)
+            shape, zone = [n, n], [0, 1, 0, 1, 0, 0]
+        r = RefSolver(dim, shape, zone, inter_method=im, flux_method=fm, n_case=ncase, cfl=0.5, periodic=periodic,
+                      diff_method=1)
+        r.cons = cons
+        rhs = r.rhs()
+        dt = r.max_dt()
+        linf = r.solve(dt)
+        out[f"c{k}_cons"] = cons
+        out[f"c{k}_rhs"] = rhs
+        out[f"c{k}_step"] = r.cons
+        out[f"c{k}_dt"] = np.array([dt, linf])
+        meta.append([k, dim, n, im, fm, ncase, int(periodic)])
+        r.close()
+    out["meta"] = np.array(meta)
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["rhs_trad6"]:
+        np.savez_compressed(HERE / "rhs_trad6.npz", **rhs_trad6(np.random.default_rng(606)))
+        return
     rng = np.random.default_rng(20261203)
     (HERE / "sod_congtcns5ct5_101.json").write_text(json.dumps(sod_log(), indent=0))
     (HERE / "order_congfd.json").write_text(json.dumps(order_txt(), indent=1))
@@ -190,6 +235,7 @@ def main():
     np.savez_compressed(HERE / "rhs_2d.npz", **rhs_2d(rng))
     np.savez_compressed(HERE / "sod_400.npz", **sod_400())
     np.savez_compressed(HERE / "kat_face.npz", **kat_face(np.random.default_rng(77)))
+    np.savez_compressed(HERE / "rhs_trad6.npz", **rhs_trad6(np.random.default_rng(606)))
     for p in sorted(HERE.glob("*")):
         if p.suffix in (".npz", ".json"):
             print(p.name, p.stat().st_size)

@@ -43,7 +43,8 @@ def _cfg(**kw):
 
 
 @pytest.mark.parametrize("field,value,code", [
-    ("n_ghost", 3, -6), ("gamma", 1.3, -6), ("diff_method", 1, -6), ("precision", 7, -1),
+    ("n_ghost", 3, -6), ("gamma", 1.3, -6), ("diff_method", 1, -6), ("diff_method", 2, -6), ("diff_method", 0, -6),
+    ("precision", 7, -1),
     ("dim", 4, -1), ("inter_method", 99, -6), ("flux_method", 5, -1),
 ])
 def test_config_validation_without_gpu(field, value, code):
@@ -51,6 +52,17 @@ def test_config_validation_without_gpu(field, value, code):
     h = C.c_void_p()
     assert lib.cfd_create(C.byref(cfg), C.byref(h)) == code
     assert not h.value
+
+
+def test_trad6_needs_five_ghosts_and_fp64():
+    """TRAD6 (diff_method 1) with n_ghost 4 or the mixed form is refused before
+    any device call; with n_ghost 5 in FP64 it passes validation (and then
+    needs a device)."""
+    lib, cfg = _cfg(diff_method=1, n_ghost=5, precision=1)
+    h = C.c_void_p()
+    assert lib.cfd_create(C.byref(cfg), C.byref(h)) == -6
+    lib, cfg = _cfg(diff_method=3, n_ghost=5)
+    assert lib.cfd_create(C.byref(cfg), C.byref(h)) == -6
 
 
 def test_small_grid_rejected():

@@ -26,6 +26,8 @@ def test_info_defaults_and_grid():
     assert info.icMax() == [400, 1, 1]
     assert info.geth(0) == (0.5 - -0.5) / 400 and info.geth(1) == info.geth(0)
     assert info.nGhostCell() == 4
+    info.diffMethod = zone.DiffMethod.TRAD6
+    assert info.nGhostCell() == 5  # info.cpp:10
 
 
 def test_default_bc_types_follow_initializer():

@@ -133,3 +133,23 @@ def test_reference_cross_check_random(orc, ref):
             r.cons = c
             o = OracleC(2, [n, n], 1.0 / n, im, fm)
             np.testing.assert_array_equal(o.rhs(c), r.rhs())
+
+
+def test_trad6_bitwise(orc):
+    """TRAD6 (ExplicitDif6, 5 ghosts): the C restatement against the reference's
+    own RHS, CFL step and RK3 step, 1D and 2D (tests/golden/rhs_trad6.npz)."""
+    g = np.load(GOLD / "rhs_trad6.npz")
+    bc_1d = {0: [[ORC_OUTLET] * 2] * 3, 4: [[ORC_SYMMETRY] * 2] * 3}
+    for k, dim, n, im, fm, ncase, periodic in g["meta"]:
+        if periodic:
+            bc = [[ORC_WRAP] * 2] * 3
+        else:
+            bc = bc_1d[int(ncase)] if dim == 1 else BC_OF_CASE[int(ncase)]
+        shape = [n] if dim == 1 else [n, n]
+        o = OracleC(int(dim), shape, 1.0 / n, int(im), int(fm), bc=bc, trad6=True)
+        o.cons = g[f"c{k}_cons"]
+        np.testing.assert_array_equal(o.rhs(), g[f"c{k}_rhs"], err_msg=f"case {k}")
+        dt, linf = g[f"c{k}_dt"]
+        assert o.max_dt(0.5) == dt
+        assert o.solve(dt) == linf
+        np.testing.assert_array_equal(o.cons, g[f"c{k}_step"], err_msg=f"case {k}")
