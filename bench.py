@@ -222,16 +222,8 @@ def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
     (segment recomputation + transposed stage Jacobians)."""
     import torch
     from cfd_inwsl_b200 import _lib, zone
-    rng = np.random.default_rng(seed)
-    k = np.fft.fftfreq(n, d=1.0 / n)
-    KX, KY = np.meshgrid(k, k)
-    noise = rng.normal(size=(n, n))
-    filt = np.exp(-0.5 * (2 * np.pi * 0.05) ** 2 * (KX ** 2 + KY ** 2))
-    drho = np.real(np.fft.ifft2(np.fft.fft2(noise) * filt))
-    drho *= 1e-2 / np.sqrt(np.mean(drho ** 2))
-    rho = 1.0 + drho.reshape(-1)
-    gamma = 1.4
-    cons = np.stack([rho, 0.5 * rho, 0.3 * rho, (1 / gamma) / (gamma - 1) + 0.5 * rho * (0.25 + 0.09)], -1)
+    from cfd_inwsl_b200.cases import adjoint_problem
+    cons, probes = adjoint_problem(n, seed)
     info = zone.Info()
     info.dim = 2
     info.iMax = [n + 1, n + 1, 1]
@@ -244,7 +236,6 @@ def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
     _lib.check(s.lib.cfd_set_stream(s.h, C.c_void_p(stream.cuda_stream)), s.h)
     s.set_cons(cons)
     dt = s.getTimeIntervalExplicit()
-    probes = rng.choice(n * n, 64, replace=False)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def timed(fn):

@@ -55,3 +55,22 @@ def riemann_quadrants(n, rng):
     X, Y = np.meshgrid((np.arange(n) + 0.5) / n, (np.arange(n) + 0.5) / n)
     q = (X >= 0.5).astype(int) + 2 * (Y >= 0.5).astype(int)
     return prim_to_cons(P[q].reshape(-1, 4))
+
+
+def adjoint_problem(n=256, seed=0, nprobe=64):
+    """Adjoint configuration on the periodic [0,1]^2, n^2 cells: rho = 1 + drho
+    with drho seeded Gaussian noise periodically filtered to correlation length
+    0.05 and scaled to RMS 1e-2, p = 1/gamma, (u, v) = (0.5, 0.3). Returns the
+    AoS cons and nprobe seeded probe cells (the objective is the sum of rho^2
+    over them)."""
+    rng = np.random.default_rng(seed)
+    k = np.fft.fftfreq(n, d=1.0 / n)
+    KX, KY = np.meshgrid(k, k)
+    noise = rng.normal(size=(n, n))
+    filt = np.exp(-0.5 * (2 * np.pi * 0.05) ** 2 * (KX ** 2 + KY ** 2))
+    drho = np.real(np.fft.ifft2(np.fft.fft2(noise) * filt))
+    drho *= 1e-2 / np.sqrt(np.mean(drho ** 2))
+    rho = 1.0 + drho.reshape(-1)
+    cons = np.stack([rho, 0.5 * rho, 0.3 * rho, (1 / GAMMA) / (GAMMA - 1) + 0.5 * rho * (0.25 + 0.09)], -1)
+    probes = rng.choice(n * n, nprobe, replace=False)
+    return cons, probes

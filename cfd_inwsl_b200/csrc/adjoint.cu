@@ -1,11 +1,13 @@
 // Discrete adjoint of one RHS evaluation (cfd_rhs_vjp, cfd_adjoint_*), fast
-// flavour (FMA), 2D Euler, WCNS5 + Roe + MND6, periodic in both directions.
+// flavour (FMA), 2D Euler, WCNS5 or TENO (frozen cut-off) + Roe + MND6,
+// periodic in both directions.
 //
 // The forward path per line (SpDistributor::rhsSolve, sp_distributor.cpp:3-79):
 //   face j (x_{j-1/2}), stencil cells j-3..j+2:
 //     Roe average of cells j-1, j           (eigensystemEuler2D, eigenSystem.cpp:13-86)
 //     q_k = L_k . U for the six cells        (primToChar, eigenSystem.cpp:88-123)
-//     QL_k = W(q_k[0..4]), QR_k = W(q_k[5..1]) (weno5_JSchen, interScheme.hpp:17-45)
+//     QL_k = W(q_k[0..4]), QR_k = W(q_k[5..1]) (weno5_JSchen, interScheme.hpp:17-45, or a
+//                                            TENO stencil with its flag frozen, adjoint_math.h)
 //     face cons R QL / R QR, then prims, positivity fallback
 //                                            (Recon5Order2DEulerEig::reconI, reconstructor5order.hpp:246-356)
 //     F_j = Roe(face prims)                  (roeFlux2DSym, fluxSchemes.hpp:420-553)
@@ -28,9 +30,9 @@ namespace {
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 // one thread per face: P[(m * 4 + v) * ncell + cell(face)] = d(mu . R)/dU of stencil cell m
-template <int AX>
+template <int AX, int FAM>
 __global__ void face_vjp_kernel(const double *__restrict__ u, const double *__restrict__ mu, double *__restrict__ P,
-                                int nx, int ny, double inv_h)
+                                int nx, int ny, double inv_h, double ct)
 {
     const long long ncell = (long long)nx * ny;
     const int nd = (AX == 0) ? nx : ny;
@@ -58,7 +60,7 @@ __global__ void face_vjp_kernel(const double *__restrict__ u, const double *__re
         for (int v = 0; v < 4; v++)
             Fb[v] = (kW0 * (mu[v * ncell + cm1] - mu[v * ncell + c0]) +
                      kW2 * (mu[v * ncell + cm2] - mu[v * ncell + cp1])) * inv_h;
-        face_vjp<AX>(U, Fb, Ub);
+        face_vjp<AX>(U, Fb, Ub, FAM, ct);
 #pragma unroll
         for (int m = 0; m < 6; m++)
 #pragma unroll
@@ -120,18 +122,34 @@ unsigned grid_for(long long n, int threads)
 
 } // namespace
 
-cudaError_t launch_sweep_vjp(int axis, const double *u, const double *mu, double *lam, double *P, int nx, int ny,
-                             double h, bool accumulate, cudaStream_t st)
+template <int AX>
+cudaError_t launch_faces(int fam, double ct, const double *u, const double *mu, double *P, int nx, int ny,
+                         double inv_h, cudaStream_t st)
+{
+    const long long ncell = (long long)nx * ny;
+    if (fam == ADJ_WCNS5)
+        face_vjp_kernel<AX, ADJ_WCNS5><<<grid_for(ncell, 128), 128, 0, st>>>(u, mu, P, nx, ny, inv_h, ct);
+    else if (fam == ADJ_TENOZ)
+        face_vjp_kernel<AX, ADJ_TENOZ><<<grid_for(ncell, 128), 128, 0, st>>>(u, mu, P, nx, ny, inv_h, ct);
+    else if (fam == ADJ_TENOCONG)
+        face_vjp_kernel<AX, ADJ_TENOCONG><<<grid_for(ncell, 128), 128, 0, st>>>(u, mu, P, nx, ny, inv_h, ct);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_vjp(int axis, int fam, double ct, const double *u, const double *mu, double *lam, double *P,
+                             int nx, int ny, double h, bool accumulate, cudaStream_t st)
 {
     const long long ncell = (long long)nx * ny;
     const double inv_h = 1.0 / h;
-    if (axis == 0) {
-        face_vjp_kernel<0><<<grid_for(ncell, 128), 128, 0, st>>>(u, mu, P, nx, ny, inv_h);
+    cudaError_t e = axis == 0 ? launch_faces<0>(fam, ct, u, mu, P, nx, ny, inv_h, st)
+                              : launch_faces<1>(fam, ct, u, mu, P, nx, ny, inv_h, st);
+    if (e != cudaSuccess) return e;
+    if (axis == 0)
         gather_kernel<0><<<grid_for(ncell, 256), 256, 0, st>>>(u, mu, P, lam, nx, ny, inv_h, accumulate ? 1 : 0);
-    } else {
-        face_vjp_kernel<1><<<grid_for(ncell, 128), 128, 0, st>>>(u, mu, P, nx, ny, inv_h);
+    else
         gather_kernel<1><<<grid_for(ncell, 256), 256, 0, st>>>(u, mu, P, lam, nx, ny, inv_h, accumulate ? 1 : 0);
-    }
     return cudaGetLastError();
 }
 

@@ -1,7 +1,7 @@
 // Launchers of the discrete-adjoint kernels (adjoint.cu, fast flavour).
 //
 // The adjoint differentiates one RHS evaluation of the 2D Euler path with
-// WCNS5 (weno5_JSchen) characteristic reconstruction, the Roe flux
+// WCNS5 (weno5_JSchen) or TENO (cut-off frozen) characteristic reconstruction, the Roe flux
 // (roeFlux2DSym) and the MND6 difference on a grid periodic in both
 // directions: lam = (dR/dU)^T mu, R the RHS of SpDistributor::rhsSolve.
 #pragma once
@@ -11,10 +11,11 @@ namespace cfd {
 namespace adj {
 
 // One direction's share of lam = (dR/dU)^T mu, all arrays planar SoA
-// [4][nx*ny]. P is scratch of 24 * nx * ny doubles (per-face contributions).
+// [4][nx*ny]. fam: interpolation family (0 WCNS5, 2 TENO-Z, 3 TENO-Cong) with
+// constant ct. P is scratch of 24 * nx * ny doubles (per-face contributions).
 // accumulate = false overwrites lam, true adds to it.
-cudaError_t launch_sweep_vjp(int axis, const double *u, const double *mu, double *lam, double *P, int nx, int ny,
-                             double h, bool accumulate, cudaStream_t st);
+cudaError_t launch_sweep_vjp(int axis, int fam, double ct, const double *u, const double *mu, double *lam, double *P,
+                             int nx, int ny, double h, bool accumulate, cudaStream_t st);
 
 // y = a * x + b * y over n doubles
 cudaError_t launch_axpby(double a, const double *x, double b, double *y, long long n, cudaStream_t st);

@@ -1,8 +1,13 @@
 // Discrete-adjoint arithmetic of one face and one node of the 2D Euler path
-// (WCNS5 characteristic reconstruction, Roe flux, node fluxes), host and
-// device: adjoint.cu runs it on the GPU, and the CPU tests compile it with the
-// host compiler to check every vector-Jacobian product against extended-
+// (WCNS5 or TENO characteristic reconstruction, Roe flux, node fluxes), host
+// and device: adjoint.cu runs it on the GPU, and the CPU tests compile it with
+// the host compiler to check every vector-Jacobian product against extended-
 // precision finite differences of the same forward formulas.
+//
+// TENO's cut-off decision is a step function of the stencil values. The
+// adjoint freezes it: the flag of the forward state selects one of the eight
+// fixed linear stencils (interScheme.hpp:445-480), and the derivative of the
+// interpolation is that stencil's coefficients.
 #pragma once
 #include <cmath>
 
@@ -86,6 +91,85 @@ ADJ_HD void wcns5_adj(const double *q, double Qb, double *qb)
     qb[2] += ab0 + 3.0 * bq0 - 2.0 * ab1 + ab2 + 3.0 * bq2 + 1.875 * ub0 + 0.75 * ub1 + 0.375 * ub2;
     qb[3] += ab1 - bq1 - 2.0 * ab2 - 4.0 * bq2 + 0.375 * ub1 + 0.75 * ub2;
     qb[4] += ab2 + bq2 - 0.125 * ub2;
+}
+
+// Interpolations the adjoint differentiates (the library's family numbers).
+enum AdjInterp : int { ADJ_WCNS5 = 0, ADJ_TENOZ = 2, ADJ_TENOCONG = 3 };
+
+// Coefficients of the fixed stencil a TENO flag selects (bit k: stencil k cut).
+template <class T>
+ADJ_HD void teno_coeffs(unsigned flag, T *a)
+{
+    for (int m = 0; m < 5; m++) a[m] = T(0);
+    switch (flag & 7u) {
+    case 0: a[0] = T(3) / 128; a[1] = T(-5) / 32; a[2] = T(45) / 64; a[3] = T(15) / 32; a[4] = T(-5) / 128; break;
+    case 1: a[1] = T(-1) / 16; a[2] = T(9) / 16; a[3] = T(9) / 16; a[4] = T(-1) / 16; break;
+    case 2:
+    case 3: a[2] = T(3) / 8; a[3] = T(3) / 4; a[4] = T(-1) / 8; break;
+    case 4: a[0] = T(1) / 16; a[1] = T(-5) / 16; a[2] = T(15) / 16; a[3] = T(5) / 16; break;
+    case 5: a[1] = T(-1) / 8; a[2] = T(3) / 4; a[3] = T(3) / 8; break;
+    case 6: a[0] = T(3) / 8; a[1] = T(-5) / 4; a[2] = T(15) / 8; break;
+    default: a[2] = T(1); break;
+    }
+}
+
+// The cut-off flag of the stencil q[0..4]: Teno5_Z (interScheme.hpp:384-452),
+// measure_k = (1 + tau / (beta_k + 1e-40))^6 cut below ct * sum_j measure_j;
+// Teno5_CongZ (interScheme.hpp:494-584), cut where
+// tau beta_min < (ct tau - (1 - ct) beta_min) beta_k.
+template <class T>
+ADJ_HD unsigned teno_flag(int fam, const T *q, double ct)
+{
+    const T a0 = q[0] - 2 * q[1] + q[2], b0 = q[0] - 4 * q[1] + 3 * q[2];
+    const T a1 = q[1] - 2 * q[2] + q[3], b1 = q[1] - q[3];
+    const T a2 = q[2] - 2 * q[3] + q[4], b2 = 3 * q[2] - 4 * q[3] + q[4];
+    const T be[3] = {a0 * a0 + T(0.25) * b0 * b0, a1 * a1 + T(0.25) * b1 * b1, a2 * a2 + T(0.25) * b2 * b2};
+    const T tau = be[2] > be[0] ? be[2] - be[0] : be[0] - be[2];
+    unsigned flag = 0;
+    if (fam == ADJ_TENOZ) {
+        T m[3], sum = T(0);
+        for (int k = 0; k < 3; k++) {
+            T t = T(1) + tau / (be[k] + T(1e-40));
+            t *= t;
+            m[k] = t * t * t;
+            sum += m[k];
+        }
+        for (int k = 0; k < 3; k++)
+            if (m[k] < T(ct) * sum) flag += 1u << k;
+    } else {
+        T bmin = be[0];
+        if (be[1] < bmin) bmin = be[1];
+        if (be[2] < bmin) bmin = be[2];
+        const T rr = T(ct) * tau - (T(1) - T(ct)) * bmin, ll = tau * bmin;
+        for (int k = 0; k < 3; k++)
+            if (ll < rr * be[k]) flag += 1u << k;
+    }
+    return flag;
+}
+
+// One interpolation of family fam (constant ct) and its frozen flag.
+ADJ_HD double interp5(int fam, const double *q, double ct, unsigned &flag)
+{
+    if (fam == ADJ_WCNS5) {
+        flag = 0;
+        return wcns5(q);
+    }
+    flag = teno_flag(fam, q, ct);
+    double a[5];
+    teno_coeffs(flag, a);
+    return a[0] * q[0] + a[1] * q[1] + a[2] * q[2] + a[3] * q[3] + a[4] * q[4];
+}
+
+// qb += (dQ/dq)^T Qb with the forward's flag
+ADJ_HD void interp5_adj(int fam, const double *q, unsigned flag, double Qb, double *qb)
+{
+    if (fam == ADJ_WCNS5) {
+        wcns5_adj(q, Qb, qb);
+        return;
+    }
+    double a[5];
+    teno_coeffs(flag, a);
+    for (int m = 0; m < 5; m++) qb[m] += a[m] * Qb;
 }
 
 // Lb += (dRoe/dL)^T resb, Rb likewise (L, R: face prims)
@@ -212,9 +296,11 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
     Rb[0] += rrb; Rb[1] += vrb[0]; Rb[2] += vrb[1]; Rb[3] += prb;
 }
 
-// Forward face flux of stencil U[6][4] and Ub += (dF/dU)^T Fb.
+// Forward face flux of stencil U[6][4] and Ub += (dF/dU)^T Fb; interpolation
+// family fam (AdjInterp) with constant ct.
 template <int AX>
-ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][4])
+ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][4], int fam = ADJ_WCNS5,
+                     double ct = 0.0)
 {
     constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
     double P2[4], P3[4];
@@ -241,14 +327,15 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
     R[0][3] = 1.0; R[1][3] = u + nx * c; R[2][3] = v + ny * c; R[3][3] = h + ek + Vn * c;
 
     double q[4][6], QL[4], QR[4];
+    unsigned flL[4], flR[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
 #pragma unroll
         for (int j = 0; j < 6; j++)
             q[k][j] = L[k][0] * U[j][0] + L[k][1] * U[j][1] + L[k][2] * U[j][2] + L[k][3] * U[j][3];
         const double qm[5] = {q[k][5], q[k][4], q[k][3], q[k][2], q[k][1]};
-        QL[k] = wcns5(q[k]);
-        QR[k] = wcns5(qm);
+        QL[k] = interp5(fam, q[k], ct, flL[k]);
+        QR[k] = interp5(fam, qm, ct, flR[k]);
     }
     double cl[4], cr[4], fl[4], fr[4];
 #pragma unroll
@@ -288,10 +375,10 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
 #pragma unroll
         for (int i = 0; i < 4; i++) Rb[i][k] = QL[k] * clb[i] + QR[k] * crb[i];
         double qb[6] = {0, 0, 0, 0, 0, 0};
-        wcns5_adj(q[k], QLb, qb);
+        interp5_adj(fam, q[k], flL[k], QLb, qb);
         const double qm[5] = {q[k][5], q[k][4], q[k][3], q[k][2], q[k][1]};
         double qmb[5] = {0, 0, 0, 0, 0};
-        wcns5_adj(qm, QRb, qmb);
+        interp5_adj(fam, qm, flR[k], QRb, qmb);
         qb[5] += qmb[0]; qb[4] += qmb[1]; qb[3] += qmb[2]; qb[2] += qmb[3]; qb[1] += qmb[4];
 #pragma unroll
         for (int m = 0; m < 4; m++) {
@@ -437,8 +524,18 @@ ADJ_HD void roe_t(const T *L, const T *R, T *res)
     for (int i = 0; i < 4; i++) res[i] = T(0.5) * (Fc[i] - Fd[i]);
 }
 
+// interp5 in the generic type (flag from the same decision in T)
+template <class T>
+ADJ_HD T interp5_t(int fam, const T *q, double ct)
+{
+    if (fam == ADJ_WCNS5) return wcns5_t(q);
+    T a[5];
+    teno_coeffs(teno_flag(fam, q, ct), a);
+    return a[0] * q[0] + a[1] * q[1] + a[2] * q[2] + a[3] * q[3] + a[4] * q[4];
+}
+
 template <class T, int AX>
-ADJ_HD void face_flux_t(const T (&U)[6][4], T *F)
+ADJ_HD void face_flux_t(const T (&U)[6][4], T *F, int fam = ADJ_WCNS5, double ct = 0.0)
 {
     using std::sqrt;
     const T nx = T(AX == 0 ? 1 : 0), ny = T(AX == 1 ? 1 : 0);
@@ -468,8 +565,8 @@ ADJ_HD void face_flux_t(const T (&U)[6][4], T *F)
         T q[6];
         for (int j = 0; j < 6; j++) q[j] = L[k][0] * U[j][0] + L[k][1] * U[j][1] + L[k][2] * U[j][2] + L[k][3] * U[j][3];
         const T qm[5] = {q[5], q[4], q[3], q[2], q[1]};
-        QL[k] = wcns5_t(q);
-        QR[k] = wcns5_t(qm);
+        QL[k] = interp5_t(fam, q, ct);
+        QR[k] = interp5_t(fam, qm, ct);
     }
     T cl[4], cr[4], fl[4], fr[4];
     for (int i = 0; i < 4; i++) {

@@ -1470,9 +1470,11 @@ namespace {
 
 int adjoint_supported(cfd_handle *h)
 {
-    if (h->dim != 2 || h->fam != cfd::FAM_WCNS5 || h->cfg.flux_method != CFD_FLUX_ROE ||
-        h->cfg.precision != CFD_PREC_FP64 || h->cfg.source_type != 0 || h->cfg.diff_method != CFD_DIFF_MND6)
-        return fail(h, CFD_ERR_UNSUPPORTED, "the adjoint covers 2D WCNS5 + Roe + MND6, FP64, without source terms");
+    const bool fam_ok = h->fam == cfd::FAM_WCNS5 || h->fam == cfd::FAM_TENOZ || h->fam == cfd::FAM_TENOCONG;
+    if (h->dim != 2 || !fam_ok || h->cfg.flux_method != CFD_FLUX_ROE || h->cfg.precision != CFD_PREC_FP64 ||
+        h->cfg.source_type != 0 || h->cfg.diff_method != CFD_DIFF_MND6)
+        return fail(h, CFD_ERR_UNSUPPORTED,
+                    "the adjoint covers 2D WCNS5 / TENO-Z / TENO-Cong + Roe + MND6, FP64, without source terms");
     for (int d = 0; d < 2; d++)
         for (int sd = 0; sd < 2; sd++)
             if (h->cfg.bc[d][sd] != CFD_BND_PERIODIC_WRAP)
@@ -1499,8 +1501,8 @@ int rhs_vjp(cfd_handle *h, const double *U, const double *mu, double *w)
 {
     const int nx = h->cfg.n[0], ny = h->cfg.n[1];
     for (int d = 0; d < 2; d++) {
-        cudaError_t e =
-            cfd::adj::launch_sweep_vjp(d, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[d], d > 0, h->stream);
+        cudaError_t e = cfd::adj::launch_sweep_vjp(d, h->fam, h->icst, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[d],
+                                                   d > 0, h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
         h->launches += 2;
     }

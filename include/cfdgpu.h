@@ -238,9 +238,12 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
 /* Discrete adjoint. The reference has no adjoint; these entry points serve
  * gradient studies of the same discretisation (sensitivity of a functional of
  * the final state to the initial state). They cover 2D handles with WCNS5
- * (weno5_JSchen) reconstruction, the Roe flux, FP64, no source term and
- * CFD_BND_PERIODIC_WRAP on every side (CFD_ERR_UNSUPPORTED otherwise); the
- * positivity fallback is differentiated where it fires.
+ * (weno5_JSchen), TENO-Z (Teno5_Z family) or TENO-Cong reconstruction, the
+ * Roe flux, MND6, FP64, no source term and CFD_BND_PERIODIC_WRAP on every side
+ * (CFD_ERR_UNSUPPORTED otherwise); the positivity fallback is differentiated
+ * where it fires. TENO's cut-off decisions are frozen: each face interpolates
+ * with the fixed stencil its forward state selects, and the derivative is
+ * that stencil's.
  *
  * cfd_rhs_vjp: lam = (dR/dU)^T mu at the handle's current state, R the RHS of
  * cfd_rhs (SpDistributor::rhsSolve, sp_distributor.cpp:3-79); mu and lam are

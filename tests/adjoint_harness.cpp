@@ -35,6 +35,33 @@ void h_roe_vjp(int ax, const double *L, const double *R, const double *Fb, doubl
     if (ax == 0) roe_vjp<0>(L, R, Fb, Lb, Rb);
     else roe_vjp<1>(L, R, Fb, Lb, Rb);
 }
+void h_face_fwd_f(int ax, int fam, double ct, const long double *u, long double *F)
+{
+    long double U[6][4];
+    for (int j = 0; j < 6; j++)
+        for (int v = 0; v < 4; v++) U[j][v] = u[4 * j + v];
+    if (ax == 0) face_flux_t<long double, 0>(U, F, fam, ct);
+    else face_flux_t<long double, 1>(U, F, fam, ct);
+}
+void h_face_vjp_f(int ax, int fam, double ct, const double *u, const double *Fb, double *ub)
+{
+    double U[6][4], Ub[6][4] = {};
+    for (int j = 0; j < 6; j++)
+        for (int v = 0; v < 4; v++) U[j][v] = u[4 * j + v];
+    if (ax == 0) face_vjp<0>(U, Fb, Ub, fam, ct);
+    else face_vjp<1>(U, Fb, Ub, fam, ct);
+    for (int j = 0; j < 6; j++)
+        for (int v = 0; v < 4; v++) ub[4 * j + v] = Ub[j][v];
+}
+unsigned h_teno_flag(int fam, const double *q, double ct) { return teno_flag(fam, q, ct); }
+long double h_interp_fwd(int fam, const long double *q, double ct) { return interp5_t(fam, q, ct); }
+void h_interp_vjp(int fam, const double *q, double ct, double Qb, double *qb)
+{
+    unsigned flag;
+    for (int i = 0; i < 5; i++) qb[i] = 0.0;
+    interp5(fam, q, ct, flag);
+    interp5_adj(fam, q, flag, Qb, qb);
+}
 long double h_wcns5_fwd(const long double *q) { return wcns5_t(q); }
 void h_wcns5_vjp(const double *q, double Qb, double *qb)
 {

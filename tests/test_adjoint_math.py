@@ -5,6 +5,10 @@ hand-written vector-Jacobian product (WCNS5 interpolation, Roe flux, node
 flux, the whole face: projection, interpolation, back projection, Roe) is
 checked entry by entry against central finite differences of the same forward
 formulas evaluated in long double. Tolerance 1e-6 relative to the Jacobian row.
+TENO interpolations (TENO-Z, cut-off 1e-5; TENO-Cong, CT of Teno5_CongZ) are
+differentiated with the cut-off decision frozen at the evaluation point; the
+stencils below are away from decision boundaries, so finite differences see
+the same selection.
 """
 import ctypes as C
 import shutil
@@ -28,6 +32,13 @@ def harness(tmp_path_factory):
                     str(ROOT / "tests" / "adjoint_harness.cpp"), "-o", str(out)], check=True)
     lib = C.CDLL(str(out))
     lib.h_wcns5_fwd.restype = LD
+    lib.h_interp_fwd.restype = LD
+    lib.h_interp_fwd.argtypes = [C.c_int, C.c_void_p, C.c_double]
+    lib.h_interp_vjp.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    lib.h_teno_flag.restype = C.c_uint
+    lib.h_teno_flag.argtypes = [C.c_int, C.c_void_p, C.c_double]
+    lib.h_face_fwd_f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+    lib.h_face_vjp_f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     return lib
 
 
@@ -149,3 +160,62 @@ def test_face_vjp(harness, ax, kind):
         return np.array(list(ub))
 
     check_rows(J, row)
+
+
+TENOZ, TENOCONG = 2, 3
+CT = {TENOZ: 1e-5, TENOCONG: 0.15704178024750198}
+
+
+@pytest.mark.parametrize("fam", [TENOZ, TENOCONG])
+def test_teno_frozen_interpolation(harness, fam):
+    """The frozen-flag TENO derivative is the selected stencil's coefficients;
+    the stencils cover kept-all, one-cut and two-cut selections."""
+    rng = np.random.default_rng(fam)
+    seen = set()
+    qs = [rng.normal(size=5) for _ in range(40)]
+    # jumps with generic values (no smoothness indicator exactly zero: those
+    # sit on a decision boundary)
+    qs += [np.array([0.1, 0.12, 0.13, 1.0, 1.05]), np.array([1.0, 1.02, 0.1, 0.11, 0.125]),
+           np.array([0.2, 0.21, 1.0, 1.03, 1.01]), np.array([1, 2, 3.1, 4, 5.2]),
+           np.array([0.05, 0.0, 0.02, 0.01, 1.0])]
+    for q in qs:
+        flag = harness.h_teno_flag(fam, dbl(q), CT[fam])
+        seen.add(flag)
+        J = fd_jacobian(lambda x: [harness.h_interp_fwd(fam, ld(x), C.c_double(CT[fam]))], q, 1)
+        qb = (C.c_double * 5)()
+        harness.h_interp_vjp(fam, dbl(q), C.c_double(CT[fam]), C.c_double(1.0), qb)
+        assert np.abs(J[0] - np.array(qb)).max() <= 1e-7 * np.abs(J[0]).max(), (q, flag, J[0], list(qb))
+    assert 0 in seen and len(seen) >= 3, seen
+
+
+@pytest.mark.parametrize("ax", [0, 1])
+@pytest.mark.parametrize("fam", [TENOZ, TENOCONG])
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+def test_face_vjp_teno(harness, ax, fam, kind):
+    rng = np.random.default_rng(20 + ax + 2 * fam)
+    x = np.linspace(0, 1, 6)
+    for trial in range(3):
+        if kind == "smooth":
+            ph = rng.uniform(0, 6)
+            prims = [[1 + 0.2 * np.sin(3 * xi + ph), 0.5 + 0.1 * np.cos(2 * xi + ph), 0.3 + 0.05 * xi,
+                      0.7 + 0.1 * np.sin(xi + ph)] for xi in x]
+        else:
+            prims = [[rng.uniform(0.5, 1.5), rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5), rng.uniform(0.5, 1.5)]
+                     for _ in x]
+        U6 = sum((prim_to_cons(p) for p in prims), [])
+
+        def f(xx):
+            out = (LD * 4)()
+            harness.h_face_fwd_f(ax, fam, CT[fam], ld(xx), out)
+            return list(out)
+
+        J = fd_jacobian(f, U6, 4)
+
+        def row(k):
+            Fb = np.zeros(4)
+            Fb[k] = 1.0
+            ub = (C.c_double * 24)()
+            harness.h_face_vjp_f(ax, fam, CT[fam], dbl(U6), dbl(Fb), ub)
+            return np.array(list(ub))
+
+        check_rows(J, row)
