@@ -300,20 +300,26 @@ def batch_throughput(device, stream, ncases=256, steps=20, seed=0):
     _lib.check(b.lib.cfd_batch_set_stream(b.h, C.c_void_p(stream.cuda_stream)))
     for i, n in enumerate(sizes):
         b.set_cons(i, cases.riemann_quadrants(n, rng))
-    b.run(0.25, end_step=1, max_steps=3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    _, ns = b.run(0.25, end_step=1, max_steps=steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    cell_steps = float(sum(n * n * int(k) for n, k in zip(sizes, ns)))
+
+    def timed_run():
+        b.run(0.25, end_step=1, max_steps=3)  # warm-up (graph capture after a tiling change)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _, ns = b.run(0.25, end_step=1, max_steps=steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), float(sum(n * n * int(k) for n, k in zip(sizes, ns)))
+
+    ms0, cs0 = timed_run()  # the default tiling: whole lines, single-grid tile shapes
+    tiling = b.autotune()
+    ms, cell_steps = timed_run()
     b.close()
     return {"config": f"{ncases} cases, N = round(2^U(7,10)) (seeded, {min(sizes)}..{max(sizes)}), "
                       "WCNS5 + HLLC, CFL 0.5, transmissive, per-case dt",
             "cells": int(sum(n * n for n in sizes)), "steps_per_case": steps, "ms": ms,
-            "value": cell_steps / (ms / 1e3), "unit": "cell-steps/s"}
+            "value": cell_steps / (ms / 1e3), "unit": "cell-steps/s",
+            "autotuned_tiling": tiling, "default_tiling_value": cs0 / (ms0 / 1e3)}
 
 
 # --------------------------------------------------------------------- our arm

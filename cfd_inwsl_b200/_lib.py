@@ -83,6 +83,8 @@ _PROTOS = {
     "cfd_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_batch_launch_count": (C.c_ulonglong, [C.c_void_p]),
     "cfd_batch_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "cfd_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cfd_batch_set_tiling": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "cfd_accuracy_test": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "cfd_eval_face": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

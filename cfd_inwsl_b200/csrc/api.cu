@@ -1192,6 +1192,10 @@ struct cfd_batch {
     // work-list order: cases by decreasing cell count, so that the persistent
     // CTAs take the longest tiles first and the tail holds the short ones
     std::vector<int> order;
+    // tiling per direction, chosen by cfd_batch_autotune: tile shape (0 the
+    // single-grid shape, 1 the alternative), segments per line, one persistent
+    // CTA per SM instead of as many as fit
+    int shape[3] = {0, 0, 0}, split[3] = {1, 1, 1}, one_cta[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     unsigned long long launches = 0;
@@ -1238,6 +1242,57 @@ SweepParams batch_params(cfd_batch *b, int c, int slot, int stage, int d)
     return p;
 }
 
+// Cells per chunk of the sweep along d with the batch's tile shape.
+int batch_chunk(const cfd_batch *b, int d)
+{
+    if (b->nv == 3) return cfd::k1S;
+    if (d == 0) return b->shape[0] ? cfd::kXS2 : cfd::kXS;
+    return b->shape[d] ? cfd::kYS2 : cfd::kYS;
+}
+
+// Segment lengths of every case (lines cut into split[d] segments of whole
+// chunks) and the work list's tile prefix sums for the current tiling.
+int batch_layout(cfd_batch *b)
+{
+    std::vector<long long> ts((size_t)b->dim * (b->ncases + 1));
+    b->tile_total.assign(b->dim, 0);
+    for (int d = 0; d < b->dim; d++) {
+        const int S = batch_chunk(b, d);
+        long long acc = 0;
+        for (int i = 0; i < b->ncases; i++) {
+            cfd_handle *h = b->h[b->order[i]];
+            const int n = h->cfg.n[d];
+            int seg = (n + b->split[d] - 1) / b->split[d];
+            seg = ((seg + S - 1) / S) * S;
+            h->seg_len[d] = seg < n ? seg : n;
+            ts[(size_t)d * (b->ncases + 1) + i] = acc;
+            acc += cfd::sweep_tile_count(b->nv, d, base_params(h, d), b->shape[d]);
+        }
+        ts[(size_t)d * (b->ncases + 1) + b->ncases] = acc;
+        b->tile_total[d] = acc;
+    }
+    CFD_BCUDA(b, cudaMemcpy(b->d_tile_start, ts.data(), sizeof(long long) * ts.size(), cudaMemcpyHostToDevice));
+    if (b->graph) {  // captured with the old tiling
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return CFD_OK;
+}
+
+cfd::BatchSweep batch_sweep(cfd_batch *b, int slot, int stage, int d)
+{
+    cfd::BatchSweep bs;
+    bs.cases = b->d_params + (size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases;
+    bs.tile_start = b->d_tile_start + (size_t)d * (b->ncases + 1);
+    bs.ncases = b->ncases;
+    bs.total_tiles = b->tile_total[d];
+    bs.num_sms = b->num_sms;
+    bs.prec = b->prec;
+    bs.shape = b->shape[d];
+    bs.one_cta = b->one_cta[d];
+    return bs;
+}
+
 int batch_enqueue_step(cfd_batch *b, int slot)
 {
     int g = (b->ncases + 127) / 128;
@@ -1245,13 +1300,7 @@ int batch_enqueue_step(cfd_batch *b, int slot)
     CFD_BCUDA(b, cudaGetLastError());
     for (int stage = 1; stage <= 3; stage++) {
         for (int d = 0; d < b->dim; d++) {
-            cfd::BatchSweep bs;
-            bs.cases = b->d_params + (size_t)((slot * 3 + (stage - 1)) * b->dim + d) * b->ncases;
-            bs.tile_start = b->d_tile_start + (size_t)d * (b->ncases + 1);
-            bs.ncases = b->ncases;
-            bs.total_tiles = b->tile_total[d];
-            bs.num_sms = b->num_sms;
-            bs.prec = b->prec;
+            const cfd::BatchSweep bs = batch_sweep(b, slot, stage, d);
             cudaError_t e = cfd::launch_sweep_batched_any(b->strict, b->nv, b->fam, d, b->flux, bs, b->stream);
             if (e != cudaSuccess) return bfail(b, CFD_ERR_CUDA, std::string("batched sweep: ") + cudaGetErrorString(e));
         }
@@ -1321,21 +1370,15 @@ int cfd_batch_create(const cfd_config *cfgs, int ncases, cfd_batch **out)
     b->order.resize(ncases);
     for (int c = 0; c < ncases; c++) b->order[c] = c;
     std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->h[x]->ncell > b->h[y]->ncell; });
-    std::vector<long long> ts((size_t)b->dim * (ncases + 1));
-    b->tile_total.assign(b->dim, 0);
-    for (int d = 0; d < b->dim; d++) {
-        long long acc = 0;
-        for (int i = 0; i < ncases; i++) {
-            ts[(size_t)d * (ncases + 1) + i] = acc;
-            acc += cfd::sweep_tile_count(b->nv, d, base_params(b->h[b->order[i]], d));
-        }
-        ts[(size_t)d * (ncases + 1) + ncases] = acc;
-        b->tile_total[d] = acc;
+    // whole lines by default (cfd_batch_autotune may cut them); the config's
+    // seg_len of each case is replaced by the batch's tiling
+    if ((e = cudaMalloc(&b->d_tile_start, sizeof(long long) * b->dim * (ncases + 1))) != cudaSuccess) return bail(e);
+    int rc = batch_layout(b);
+    if (rc) {
+        fprintf(stderr, "cfd_batch_create: %s\n", b->msg.c_str());
+        cfd_batch_destroy(b);
+        return rc;
     }
-    if ((e = cudaMalloc(&b->d_tile_start, sizeof(long long) * ts.size())) != cudaSuccess) return bail(e);
-    if ((e = cudaMemcpy(b->d_tile_start, ts.data(), sizeof(long long) * ts.size(), cudaMemcpyHostToDevice)) !=
-        cudaSuccess)
-        return bail(e);
     *out = b;
     return CFD_OK;
 }
@@ -1460,6 +1503,93 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
         }
     }
     return rc;
+}
+
+int cfd_batch_set_tiling(cfd_batch *b, int idim, int shape, int segments, int one_cta)
+{
+    if (!b) return CFD_ERR_CONFIG;
+    const int d = idim - 1;
+    if (d < 0 || d >= b->dim || shape < 0 || shape > 1 || segments < 1 || segments > 64 || one_cta < 0 ||
+        one_cta > 1)
+        return bfail(b, CFD_ERR_CONFIG, "bad tiling");
+    if (shape == 1 && !(b->nv >= 4 && b->prec == 0))
+        return bfail(b, CFD_ERR_UNSUPPORTED, "the alternative tile shape is 2D/3D FP64 only");
+    b->shape[d] = shape;
+    b->split[d] = segments;
+    b->one_cta[d] = one_cta;
+    return batch_layout(b);
+}
+
+int cfd_batch_autotune(cfd_batch *b, int *choice, double *ms)
+{
+    if (!b) return CFD_ERR_CONFIG;
+    // first-stage sweeps read U^0 and write only the RHS and U^(1), both
+    // scratch between steps; step control: not done, dt = 0
+    for (int c = 0; c < b->ncases; c++) {
+        int rc = sync_bc(b->h[c]);
+        if (rc) return bfail(b, rc, b->h[c]->msg);
+    }
+    std::memset(b->ctl_host, 0, sizeof(cfd::StepCtl) * b->ncases);
+    CFD_BCUDA(b, cudaMemcpyAsync(b->ctl, b->ctl_host, sizeof(cfd::StepCtl) * b->ncases, cudaMemcpyHostToDevice,
+                                 b->stream));
+    const bool alt = b->nv >= 4 && b->prec == 0;  // the alternative shapes: 2D/3D FP64
+    cudaEvent_t e0, e1;
+    CFD_BCUDA(b, cudaEventCreate(&e0));
+    CFD_BCUDA(b, cudaEventCreate(&e1));
+    int rc = CFD_OK;
+    for (int d = 0; d < b->dim && rc == CFD_OK; d++) {
+        float best = 3.4e38f;
+        int best_cfg[3] = {b->shape[d], b->split[d], b->one_cta[d]};
+        for (int shape = 0; shape <= (alt ? 1 : 0) && rc == CFD_OK; shape++)
+            for (int split = 1; split <= 2 && rc == CFD_OK; split++)
+                for (int one = 0; one <= 1 && rc == CFD_OK; one++) {
+                    b->shape[d] = shape;
+                    b->split[d] = split;
+                    b->one_cta[d] = one;
+                    if ((rc = batch_layout(b))) break;
+                    for (int i = 0; i < b->ncases; i++)
+                        b->params_host[(size_t)d * b->ncases + i] = batch_params(b, b->order[i], 0, 1, d);
+                    const cfd::BatchSweep bs = batch_sweep(b, 0, 1, d);
+                    CFD_BCUDA(b, cudaMemcpyAsync(b->d_params + (size_t)d * b->ncases,
+                                                 b->params_host.data() + (size_t)d * b->ncases,
+                                                 sizeof(SweepParams) * b->ncases, cudaMemcpyHostToDevice, b->stream));
+                    float t = 0.0f;
+                    for (int rep = 0; rep < 4 && rc == CFD_OK; rep++) {  // one warm-up, three timed
+                        CFD_BCUDA(b, cudaEventRecord(e0, b->stream));
+                        cudaError_t e =
+                            cfd::launch_sweep_batched_any(b->strict, b->nv, b->fam, d, b->flux, bs, b->stream);
+                        if (e != cudaSuccess)
+                            rc = bfail(b, CFD_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+                        CFD_BCUDA(b, cudaEventRecord(e1, b->stream));
+                        CFD_BCUDA(b, cudaEventSynchronize(e1));
+                        float ms1 = 0.0f;
+                        CFD_BCUDA(b, cudaEventElapsedTime(&ms1, e0, e1));
+                        if (rep > 0) t += ms1;
+                    }
+                    if (rc == CFD_OK && t < best) {
+                        best = t;
+                        best_cfg[0] = shape;
+                        best_cfg[1] = split;
+                        best_cfg[2] = one;
+                    }
+                }
+        b->shape[d] = best_cfg[0];
+        b->split[d] = best_cfg[1];
+        b->one_cta[d] = best_cfg[2];
+        if (choice) {
+            choice[3 * d] = best_cfg[0];
+            choice[3 * d + 1] = best_cfg[1];
+            choice[3 * d + 2] = best_cfg[2];
+        }
+        if (ms) ms[d] = best / 3.0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc2 = batch_layout(b);
+    for (int c = 0; c < b->ncases && rc == CFD_OK; c++)
+        CFD_BCUDA(b, cudaMemsetAsync(b->h[c]->err, 0, sizeof(unsigned), b->stream));
+    CFD_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return rc ? rc : rc2;
 }
 
 } // extern "C"

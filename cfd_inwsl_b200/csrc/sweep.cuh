@@ -509,7 +509,7 @@ static cudaError_t launch_batched_shape_p(const BatchSweep &b, cudaStream_t st)
         if (blocks_per_sm[dev] < 1) blocks_per_sm[dev] = 1;
         attr_set[dev] = true;
     }
-    long long grid = (long long)b.num_sms * blocks_per_sm[dev];
+    long long grid = (long long)b.num_sms * (b.one_cta ? 1 : blocks_per_sm[dev]);
     if (b.total_tiles < grid) grid = b.total_tiles;
     if (grid <= 0) return cudaSuccess;
     sweep_batched_kernel<NV, AX, FAM, FLUX, S, W, PREC>
@@ -566,7 +566,8 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
     }
 }
 
-// Persistent batched sweep (2D and 3D; same tile shapes as launch_sweep).
+// Persistent batched sweep (1D, 2D and 3D; the tile shapes of launch_sweep or,
+// for 2D/3D FP64 with b.shape = 1, the alternative shapes).
 template <int NV, int FAM>
 cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStream_t st)
 {
@@ -575,6 +576,21 @@ cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStre
         return flux == FLUX_HLLC ? launch_batched_shape<3, 0, FAM, FLUX_HLLC, k1S, k1W>(b, st)
                                  : launch_batched_shape<3, 0, FAM, FLUX_ROE, k1S, k1W>(b, st);
     } else {
+        if (b.shape == 1) {
+            if (b.prec != 0) return cudaErrorInvalidValue;
+            if (ax == 0)
+                return flux == FLUX_HLLC ? launch_batched_shape_p<NV, 0, FAM, FLUX_HLLC, kXS2, kXW2, 0>(b, st)
+                                         : launch_batched_shape_p<NV, 0, FAM, FLUX_ROE, kXS2, kXW2, 0>(b, st);
+            if (ax == 1)
+                return flux == FLUX_HLLC ? launch_batched_shape_p<NV, 1, FAM, FLUX_HLLC, kYS2, kYW2, 0>(b, st)
+                                         : launch_batched_shape_p<NV, 1, FAM, FLUX_ROE, kYS2, kYW2, 0>(b, st);
+            if constexpr (NV == 5) {
+                if (ax == 2)
+                    return flux == FLUX_HLLC ? launch_batched_shape_p<NV, 2, FAM, FLUX_HLLC, kYS2, kYW2, 0>(b, st)
+                                             : launch_batched_shape_p<NV, 2, FAM, FLUX_ROE, kYS2, kYW2, 0>(b, st);
+            }
+            return cudaErrorInvalidValue;
+        }
         if (ax == 0)
             return flux == FLUX_HLLC ? launch_batched_shape<NV, 0, FAM, FLUX_HLLC, kXS, kXW>(b, st)
                                      : launch_batched_shape<NV, 0, FAM, FLUX_ROE, kXS, kXW>(b, st);

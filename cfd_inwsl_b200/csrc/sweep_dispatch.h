@@ -50,12 +50,13 @@ inline cudaError_t launch_sweep_batched_any(bool strict_flavour, int nv, int fam
     return cudaErrorInvalidValue;
 }
 
-// Tile count of one case's sweep along ax (same shapes as the launchers).
-inline long long sweep_tile_count(int nv, int ax, const SweepParams &p)
+// Tile count of one case's sweep along ax (same shapes as the launchers;
+// shape 1: the batched alternative shapes).
+inline long long sweep_tile_count(int nv, int ax, const SweepParams &p, int shape = 0)
 {
     int T0 = (nv == 3) ? 1 : ((ax == 0) ? 1 : 0);
     int T1 = (ax == 2) ? 1 : 2;
-    int W = (nv == 3) ? k1W : ((ax == 0) ? kXW : kYW);
+    int W = (nv == 3) ? k1W : ((ax == 0) ? (shape ? kXW2 : kXW) : (shape ? kYW2 : kYW));
     long long nseg = (p.n[ax] + p.seg_len - 1) / p.seg_len;
     return (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
 }

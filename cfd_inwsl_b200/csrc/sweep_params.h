@@ -20,6 +20,11 @@ namespace cfd {
 constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
 constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
 constexpr int k1S = 128, k1W = 1;          // 1D
+// Alternative shapes of the batched 2D/3D FP64 sweeps, picked per direction by
+// the batch autotuner: 32 threads per x line (8 lines per CTA), 16 threads per
+// y/z line (16 lines per CTA).
+constexpr int kXS2 = 32, kXW2 = 8;
+constexpr int kYS2 = 16, kYW2 = 16;
 
 
 // BndType values (zone_FD/src/include/macro.hpp:33-34) plus the 3D mirror.
@@ -110,6 +115,8 @@ struct BatchSweep {
     long long total_tiles;
     int num_sms;
     int prec;
+    int shape;      // 0: default tile shape, 1: the alternative (kXS2 x kXW2 / kYS2 x kYW2; 2D/3D FP64 only)
+    int one_cta;    // 1: one persistent CTA per SM, 0: as many as fit
 };
 
 // Block-wide max of non-negative doubles followed by one atomicMax per value.

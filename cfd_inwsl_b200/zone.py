@@ -483,6 +483,26 @@ class BlockBatch:
             info.t = float(tt)
         return t, ns
 
+    def set_tiling(self, idim: int, shape: int = 0, segments: int = 1, one_cta: bool = False):
+        """cfd_batch_set_tiling for the sweeps along idim (1-based)."""
+        rc = self.lib.cfd_batch_set_tiling(self.h, int(idim), int(shape), int(segments), int(bool(one_cta)))
+        if rc != 0:
+            m = self.lib.cfd_batch_last_error(self.h)
+            raise _lib.CfdError(rc, m.decode() if m else "")
+
+    def autotune(self) -> list[dict]:
+        """cfd_batch_autotune: per direction, the tiling it chose and the
+        chosen first-stage sweep's time."""
+        dim = self.infos[0].dim
+        choice = np.zeros(9, dtype=np.int32)
+        ms = np.zeros(3)
+        rc = self.lib.cfd_batch_autotune(self.h, _lib.ptr(choice), _lib.ptr(ms))
+        if rc != 0:
+            m = self.lib.cfd_batch_last_error(self.h)
+            raise _lib.CfdError(rc, m.decode() if m else "")
+        return [{"shape": int(choice[3 * d]), "segments_per_line": int(choice[3 * d + 1]),
+                 "one_cta_per_sm": bool(choice[3 * d + 2]), "sweep_ms": float(ms[d])} for d in range(dim)]
+
 
 def sod_1d(info: Info) -> np.ndarray:
     """Sod initial state of Initializer::solInit (initializer.cpp:87-109):

@@ -235,6 +235,21 @@ unsigned long long cfd_batch_launch_count(const cfd_batch *b);
 int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_dt, int max_steps, double *t,
                   int *nsteps);
 
+/* Autotuner of the batched sweeps (no counterpart in the reference). For each
+ * direction it times the persistent first-stage sweep of the whole batch over
+ * the tilings it can run: tile shape (0: the single-grid shape, 1: 32 threads
+ * per x line / 16 per y and z line, 2D and 3D FP64 only), lines cut into 1 or
+ * 2 segments, and one or as many persistent CTAs per SM as fit; keeps the
+ * fastest. Results are bit for bit those of any other tiling. The tuning runs
+ * sweeps on the cases' current states and touches only scratch buffers (RHS,
+ * stage state); call it between runs. choice (may be NULL) receives per
+ * direction {shape, segments, one CTA per SM}, ms (may be NULL) the chosen
+ * sweep's time per direction. */
+int cfd_batch_autotune(cfd_batch *b, int *choice, double *ms);
+/* Sets the tiling of the sweeps along idim (1/2/3) by hand: shape 0/1,
+ * segments per line (1..64), one_cta 0/1, as cfd_batch_autotune reports it. */
+int cfd_batch_set_tiling(cfd_batch *b, int idim, int shape, int segments, int one_cta);
+
 /* Discrete adjoint. The reference has no adjoint; these entry points serve
  * gradient studies of the same discretisation (sensitivity of a functional of
  * the final state to the initial state). They cover 2D handles with WCNS5

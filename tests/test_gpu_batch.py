@@ -68,3 +68,41 @@ def test_batch_equals_single_case_path():
         assert rel_linf(b.cons(i), s.cons) < 1e-13, i
         s.close()
     b.close()
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_every_tiling_gives_the_same_bits(strict):
+    """Tile shapes, segments per line and persistent grid sizes only change
+    which CTA computes a face: every tiling gives the default's bits."""
+    sizes = [40, 64, 33, 130, 17]
+    base, _ = batch_setup(sizes, strict, seed=5)
+    base.run(1e9, max_steps=5)
+    want = [base.cons(i) for i in range(len(sizes))]
+    base.close()
+    for shape in (0, 1):
+        for seg in (1, 2, 3):
+            for one in (False, True):
+                b, _ = batch_setup(sizes, strict, seed=5)
+                for idim in (1, 2):
+                    b.set_tiling(idim, shape, seg, one)
+                b.run(1e9, max_steps=5)
+                for i in range(len(sizes)):
+                    np.testing.assert_array_equal(b.cons(i), want[i], err_msg=f"{shape} {seg} {one} case {i}")
+                b.close()
+
+
+def test_autotune_keeps_results(ref):
+    """cfd_batch_autotune picks a tiling per direction; the run after it is
+    still the reference's, bit for bit (strict flavour)."""
+    sizes = [48, 100, 30, 70]
+    b, states = batch_setup(sizes, True, seed=9)
+    choice = b.autotune()
+    assert len(choice) == 2 and all(c["sweep_ms"] > 0 for c in choice)
+    t, ns = b.run(0.03)
+    for i, n in enumerate(sizes):
+        r = ref.RefSolver(2, [n, n], [0, 1, 0, 1, 0, 0], inter_method=2, flux_method=0, n_case=0, cfl=0.5)
+        r.cons = states[i]
+        dts, _ = r.run(1, 0.03)
+        assert ns[i] == len(dts)
+        np.testing.assert_array_equal(b.cons(i), r.cons, err_msg=f"case {i}")
+    b.close()
