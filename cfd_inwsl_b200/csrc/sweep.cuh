@@ -101,6 +101,10 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     }
 }
 
+#ifndef CFD_SWEEP_MINB
+#define CFD_SWEEP_MINB 2
+#endif
+
 constexpr int pow2_ceil(int x)
 {
     int r = 1;
@@ -125,23 +129,23 @@ struct SweepShape {
     // mixed form: FP32 hi/lo split of the cons ring (exact FP32 increments)
     static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
     static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
+    // Resident CTAs per SM the launch bounds ask for: 512 threads per SM in
+    // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread.
+    static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? CFD_SWEEP_MINB * (256 / NT) : CFD_SWEEP_MINB) : 1;
     // Asynchronous staging (cp.async) of each thread's global operands: the next
     // chunk's cell and the epilogue's rhs / U^0 / U^k, so that their latency
-    // hides behind the face phase. Only where two CTAs per SM still fit in the
+    // hides behind the face phase. Only where MINB CTAs per SM still fit in the
     // 228 KB of an SM (1 KB of it reserved per CTA).
     // The x sweep of a 2D/3D step is always the first direction (no epilogue
     // operands to stage), so it stages only the next chunk's cells.
     static constexpr int NSTG = (AX == 0 && NV >= 4) ? 1 : 4;
     static constexpr size_t SMEM_STAGE = sizeof(double) * NSTG * NV * NT;
-    static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= 112 * 1024;
+    static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= (MINB > 2 ? 224 / MINB : 112) * 1024;
     static constexpr bool PF_EPI = PF && NSTG == 4;
     static constexpr size_t SMEM_BYTES = SMEM_RINGS + (PF ? SMEM_STAGE : 0);
 };
 
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
-#ifndef CFD_SWEEP_MINB
-#define CFD_SWEEP_MINB 2
-#endif
 __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 {
     using SH = SweepShape<NV, AX, FAM, FLUX, S, W, PREC, DIFF>;
@@ -413,7 +417,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 }
 
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
-__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
+__global__ void __launch_bounds__(S *W, (SweepShape<NV, AX, FAM, FLUX, S, W, PREC, DIFF>::MINB))
     sweep_kernel(const __grid_constant__ SweepParams p)
 {
     sweep_tile<NV, AX, FAM, FLUX, S, W, PREC, DIFF>(p, blockIdx.x);
@@ -435,7 +439,7 @@ __host__ __device__ inline long long sweep_tiles(const SweepParams &p)
 // shared memory and runs the same tile code as sweep_kernel. Cases whose
 // device loop is done are skipped tile by tile.
 template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC>
-__global__ void __launch_bounds__(S *W, (S * W <= 256) ? CFD_SWEEP_MINB : 1)
+__global__ void __launch_bounds__(S *W, (SweepShape<NV, AX, FAM, FLUX, S, W, PREC>::MINB))
     sweep_batched_kernel(const SweepParams *__restrict__ cases, const long long *__restrict__ tile_start, int ncases)
 {
     __shared__ SweepParams sp;
@@ -541,8 +545,8 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
     return cudaErrorInvalidValue;
 }
 
-// Tile shapes (kXS x kXW along x, kYS x kYW along y/z, k1S x k1W in 1D): see
-// sweep_params.h.
+// Tile shapes (kXS x kXW along x, kYS x kYW along y/z, kYSm x kYWm for the
+// mixed form along y, k1S x k1W in 1D): see sweep_params.h.
 template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st)
 {
@@ -554,9 +558,17 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
         if (ax == 0)
             return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, kXS, kXW>(p, st)
                                      : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, kXS, kXW>(p, st);
-        if (ax == 1)
+        if (ax == 1) {
+#if defined(CFD_FAST)
+            if constexpr (FAM != FAM_RESEARCH) {
+                if (p.prec == 1 && p.diff != DIFF_TRAD6)
+                    return flux == FLUX_HLLC ? launch_sweep_shape_p<NV, 1, FAM, FLUX_HLLC, kYSm, kYWm, 1, 0>(p, st)
+                                             : launch_sweep_shape_p<NV, 1, FAM, FLUX_ROE, kYSm, kYWm, 1, 0>(p, st);
+            }
+#endif
             return flux == FLUX_HLLC ? launch_sweep_shape<NV, 1, FAM, FLUX_HLLC, kYS, kYW>(p, st)
                                      : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, kYS, kYW>(p, st);
+        }
         if constexpr (NV == 5) {
             if (ax == 2)
                 return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, kYS, kYW>(p, st)

@@ -4,9 +4,12 @@
 
 namespace cfd {
 
-// Tile shapes of the sweeps: cells per chunk (S) x lines per CTA (W).
+// Tile shapes of the sweeps: cells per chunk (S) x lines per CTA (W). CTAs of
+// 128 threads run four per SM (barriers across 4 warps instead of 8): the x
+// sweeps and the mixed form's y sweep take them; the FP64 y/z sweeps keep 32
+// lines (256 threads), which measured faster there.
 #ifndef CFD_XS
-#define CFD_XS 64
+#define CFD_XS 32
 #endif
 #ifndef CFD_XW
 #define CFD_XW 4
@@ -19,6 +22,7 @@ namespace cfd {
 #endif
 constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
 constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
+constexpr int kYSm = 8, kYWm = 16;          // along y, mixed form (single grid)
 constexpr int k1S = 128, k1W = 1;          // 1D
 // Alternative shapes of the batched 2D/3D FP64 sweeps, picked per direction by
 // the batch autotuner: 32 threads per x line (8 lines per CTA), 16 threads per
