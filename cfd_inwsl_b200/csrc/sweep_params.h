@@ -22,7 +22,13 @@ namespace cfd {
 #endif
 constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
 constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
-constexpr int kYSm = 8, kYWm = 16;          // along y, mixed form (single grid)
+#ifndef CFD_YSM
+#define CFD_YSM 8
+#endif
+#ifndef CFD_YWM
+#define CFD_YWM 16
+#endif
+constexpr int kYSm = CFD_YSM, kYWm = CFD_YWM;  // along y, mixed form (single grid)
 constexpr int k1S = 128, k1W = 1;          // 1D
 // Alternative shapes of the batched 2D/3D FP64 sweeps, picked per direction by
 // the batch autotuner: 32 threads per x line (8 lines per CTA), 16 threads per
