@@ -322,6 +322,62 @@ def batch_throughput(device, stream, ncases=256, steps=20, seed=0):
             "autotuned_tiling": tiling, "default_tiling_value": cs0 / (ms0 / 1e3)}
 
 
+def tgv_history(device, stream, n=256, steps=100, every=10):
+    """3D Taylor-Green configuration: [0,2pi]^3 periodic, n^3 cells, WCNS5 +
+    HLLC, CFL 0.5, `steps` RK3 steps in FP64 and in the mixed form. Times the
+    steps (device loop, CUDA events on the handle's stream, outside the
+    kinetic-energy reads) and records the kinetic energy sum rho |u|^2 / 2 h^3
+    every `every` steps, computed on the device from the state buffer."""
+    import torch
+    from cfd_inwsl_b200 import _lib, zone
+    from cfd_inwsl_b200.cases import tgv_state
+    c, h = tgv_state(n)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"config": f"{n}^3 periodic [0,2pi]^3, WCNS5 + HLLC, CFL 0.5, {steps} steps", "steps": steps}
+    for key, prec in (("fp64", 0), ("mixed", 1)):
+        info = zone.Info()
+        info.dim = 3
+        info.iMax = [n + 1] * 3
+        info.calZone = [0, 2 * np.pi] * 3
+        info.interMethod = 2
+        info.fluxMethod = 0
+        info.CFL = 0.5
+        info.precision = prec
+        info.device = device
+        s = zone.BlockSolver(info, periodic=True)
+        _lib.check(s.lib.cfd_set_stream(s.h, C.c_void_p(stream.cuda_stream)), s.h)
+        s.set_cons(c)
+
+        def ke():
+            ptr = C.c_void_p()
+            _lib.check(s.lib.cfd_stage_state(s.h, 1, C.byref(ptr)), s.h)
+            from cfd_inwsl_b200.slabs import _tensor
+            u = _tensor(ptr.value, (5, n ** 3), f"cuda:{device}")
+            with torch.cuda.stream(stream):
+                k = (0.5 * (u[1] ** 2 + u[2] ** 2 + u[3] ** 2) / u[0]).sum() * h ** 3
+                return float(k.item())  # on the stream that computed it
+
+        t = C.c_double(0.0)
+        ns = C.c_int(0)
+        hist, ms = [ke()], 0.0
+        for _ in range(steps // every):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _lib.check(s.lib.cfd_run(s.h, 0.5, 1, 1e300, every, C.byref(t), C.byref(ns), None, None), s.h)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            hist.append(ke())
+        s.close()
+        out[key] = {"value": n ** 3 * steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / steps,
+                    "t_end": t.value, "kinetic_energy": hist}
+    ref = np.array(out["fp64"]["kinetic_energy"])
+    out["mixed"]["ke_max_rel_dev_vs_fp64"] = float(np.max(np.abs(np.array(out["mixed"]["kinetic_energy"]) - ref) /
+                                                          ref))
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 # --------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -497,6 +553,9 @@ def run_ours(args, rank, world, local_rank):
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_throughput(local_rank, stream)
+    tgv = None
+    if not args.no_tgv and world == 1 and dim == 2:
+        tgv = tgv_history(local_rank, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -534,6 +593,8 @@ def run_ours(args, rank, world, local_rank):
         result["adjoint"] = adjoint
     if batch is not None:
         result["batch"] = batch
+    if tgv is not None:
+        result["tgv"] = tgv
     if cpu is not None:
         result["cpu_baseline"] = cpu
     solver.close()
@@ -552,6 +613,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-tgv", action="store_true", help="skip the 3D Taylor-Green throughput and energy history")
     ap.add_argument("--force-slabs", action="store_true",
                     help="run the multi-GPU slab path (halo exchange) even on one GPU (one periodic slab)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],

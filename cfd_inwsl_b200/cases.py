@@ -74,3 +74,9 @@ def adjoint_problem(n=256, seed=0, nprobe=64):
     cons = np.stack([rho, 0.5 * rho, 0.3 * rho, (1 / GAMMA) / (GAMMA - 1) + 0.5 * rho * (0.25 + 0.09)], -1)
     probes = rng.choice(n * n, nprobe, replace=False)
     return cons, probes
+
+
+def kinetic_energy(cons, h):
+    """sum over cells of rho |u|^2 / 2 h^3 (AoS 3D cons)."""
+    c = np.asarray(cons)
+    return float(np.sum(0.5 * (c[:, 1] ** 2 + c[:, 2] ** 2 + c[:, 3] ** 2) / c[:, 0]) * h ** 3)

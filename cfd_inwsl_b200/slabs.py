@@ -223,7 +223,10 @@ class SlabRank:
         with torch.cuda.stream(self.stream):
             lam = torch.tensor(self.slab.wave_speeds(), dtype=torch.float64, device=f"cuda:{self.slab.device}")
             self.dist.all_reduce(lam, op=self.dist.ReduceOp.MAX, group=self.group)
-        return dt_from_wave_speeds(lam.cpu().numpy(), self.info.dim, cfl)
+            # read back on the same stream: a copy on torch's default stream
+            # would not wait for the reduction (the streams are non-blocking)
+            lam_host = lam.cpu().numpy()
+        return dt_from_wave_speeds(lam_host, self.info.dim, cfl)
 
     def step(self, dt: float, t: float = 0.0):
         for stage in (1, 2, 3):

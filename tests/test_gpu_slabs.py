@@ -71,3 +71,34 @@ def test_fast_flavour_slabs():
     c = quadrant_state((nx, ny), rng)
     w, g = run_both(info, c, 3, 4, periodic=True)
     assert rel_linf(g, w) < 1e-13
+
+
+def test_slab_rank_one_process_matches_whole_grid():
+    """SlabRank (the multi-GPU path of bench.py) as one NCCL rank: one periodic
+    slab, its halo exchange a copy of its own rows and dt from the all-reduced
+    wave speeds read back on the slab's stream. Bit for bit against the
+    undivided grid, dt included, on a grid large enough that a read-back
+    racing the reduction would see stale values."""
+    import socket
+    import torch.distributed as dist
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        n = 512
+        info = make_info(2, [n, n], [0, 10, 0, 10, 0, 0], im=11, fm=1, strict=True, cfl=0.4)
+        from cfd_inwsl_b200.cases import isentropic_vortex
+        c = isentropic_vortex(n)[0]
+        whole = zone.BlockSolver(info, periodic=True)
+        whole.set_cons(c)
+        rank = slabs.SlabRank(info, periodic=True)
+        rank.set_cons(c)
+        for _ in range(5):
+            dt = whole.getTimeIntervalExplicit()
+            assert rank.max_dt(info.CFL) == dt
+            whole.RK3_SSP(dt)
+            rank.step(dt)
+        np.testing.assert_array_equal(rank.slab.solver.cons, whole.cons)
+    finally:
+        dist.destroy_process_group()
