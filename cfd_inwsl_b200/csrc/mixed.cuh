@@ -21,6 +21,8 @@
 //   * Roe flux: the central part (F_L + F_R) / 2 in FP64, the upwind
 //     dissipation R |Lambda| L (U_R - U_L) / 2 in FP32 from FP64 jumps; the
 //     dissipation is O(jump), small wherever the data are smooth.
+//   * HLLC flux: the upwind side's physical flux in FP64, the wave speeds and
+//     the star-state correction S_K (U*_K - U_K), which is O(jump), in FP32.
 //
 // FP32 works on increments, never on the values: every stencil value enters as
 // cons(j) - cons(2), formed from an FP32 hi/lo split of each cell's cons
@@ -533,6 +535,82 @@ __device__ __forceinline__ void roe_md_mixed(const double *L, const double *R, d
     Fd[E] = a1 * (HAvg - cAvg * VnAvg) + a3 * (HAvg + cAvg * VnAvg) + a2 * q2 + l1r * tE;
 #pragma unroll
     for (int i = 0; i < NV; i++) res[i] = 0.5 * (Fc[i] - (double)Fd[i]);
+}
+
+// HLLC (HLLCFlux2D2, fluxSchemes.hpp, as hllc_md in euler_math.cuh) with the
+// physical flux of the upwind side in FP64 and everything of size O(jump) in
+// FP32: the wave-speed estimates and the star-state correction
+// S_K (U*_K - U_K). Every term of U*_K - U_K carries the factor
+// d_K = (S* - Vn_K) / (S_K - S*), and S* - Vn_K is formed from the FP64 jumps
+// without cancellation:
+//   S* - VnL = (dp - rR (SR - VnR) dVn) / den,  S* - VnR = (dp - rL (SL - VnL) dVn) / den,
+//   den = rL (SL - VnL) - rR (SR - VnR)  (two terms of one sign).
+// The flux is continuous where the branch (SL > 0, S* > 0, SR > 0) changes,
+// so branch decisions taken in FP32 shift it only by rounding of the jump.
+template <int NV, int AX>
+__device__ __forceinline__ void hllc_md_mixed(const double *L, const double *R, double *res)
+{
+    constexpr int D = NV - 2, E = NV - 1;
+    const double n[3] = {AX == 0 ? 1.0 : 0.0, AX == 1 ? 1.0 : 0.0, AX == 2 ? 1.0 : 0.0};
+    const double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
+    const double *vl = L + 1, *vr = R + 1;
+    double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
+    if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
+    const double VnL = vl[AX], VnR = vr[AX];
+    constexpr double kg1 = kGamma / (kGamma - 1);
+    // wave speeds in FP32
+    const float g = (float)kGamma;
+    const float rlf = (float)rl, rrf = (float)rr, plf = (float)pl, prf = (float)pr;
+    const float cl = sqrtf(g * __fdividef(plf, rlf)), cr = sqrtf(g * __fdividef(prf, rrf));
+    const float dVn = (float)(VnR - VnL), dp = (float)(pr - pl);
+    const float ps0 = 0.5f * (plf + prf) - 0.25f * (rlf + rrf) * (0.5f * (cl + cr)) * dVn;
+    const float ps = fmaxf(ps0, 0.0f);
+    const float gk = (float)((kGamma + 1.0) / (2.0 * kGamma));
+    const float ql = (ps <= plf) ? 1.0f : sqrtf(1.0f + gk * (__fdividef(ps, plf) - 1.0f));
+    const float qr = (ps <= prf) ? 1.0f : sqrtf(1.0f + gk * (__fdividef(ps, prf) - 1.0f));
+    const float aL = -cl * ql, aR = cr * qr;  // SL - VnL, SR - VnR
+    const float iden = __fdividef(1.0f, rlf * aL - rrf * aR);
+    const float sL = (dp - rrf * aR * dVn) * iden;  // S* - VnL
+    const float sR = (dp - rlf * aL * dVn) * iden;  // S* - VnR
+    const float VnLf = (float)VnL, VnRf = (float)VnR;
+    const float SL = VnLf + aL, SR = VnRf + aR, Sstar = VnLf + sL;
+
+    // FP64 physical flux of one side plus `scale` times its FP32 star correction
+    auto side = [&](double r, const double *v, double p, double k, double Vn, float a, float sK, double *out,
+                    bool star, double scale, bool accumulate) {
+        const double rH = 0.5 * r * k + kg1 * p;  // rho H
+        double F[NV];
+        F[0] = r * Vn;
+#pragma unroll
+        for (int i = 0; i < D; i++) F[1 + i] = r * v[i] * Vn + p * n[i];
+        F[E] = rH * Vn;
+        float C[NV];
+#pragma unroll
+        for (int i = 0; i < NV; i++) C[i] = 0.0f;
+        if (star) {
+            const float S = (float)Vn + a;                        // S_K
+            const float delta = __fdividef(sK, a - sK);          // (S* - Vn) / (S_K - S*)
+            const float rf = (float)r;
+            C[0] = S * rf * delta;
+#pragma unroll
+            for (int i = 0; i < D; i++) C[1 + i] = S * rf * delta * ((i == AX) ? S : (float)v[i]);
+            const float UE = (float)(rH - p);
+            const float Ss = (float)Vn + sK;                      // S*
+            C[E] = S * (delta * UE + (1.0f + delta) * sK * (rf * Ss + __fdividef((float)p, a)));
+        }
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            const double f = (F[i] + (double)C[i]) * scale;
+            out[i] = accumulate ? out[i] + f : f;
+        }
+    };
+    if (SL > 0.0f) side(rl, vl, pl, kl, VnL, aL, sL, res, false, 1.0, false);
+    else if (Sstar > 0.0f) side(rl, vl, pl, kl, VnL, aL, sL, res, true, 1.0, false);
+    else if (Sstar == 0.0f) {
+        side(rl, vl, pl, kl, VnL, aL, sL, res, true, 0.5, false);
+        side(rr, vr, pr, kr, VnR, aR, sR, res, true, 0.5, true);
+    } else if (SR > 0.0f) side(rr, vr, pr, kr, VnR, aR, sR, res, true, 1.0, false);
+    else side(rr, vr, pr, kr, VnR, aR, sR, res, false, 1.0, false);
 }
 
 } // namespace cfd

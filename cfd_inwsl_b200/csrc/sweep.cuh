@@ -268,6 +268,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             }
         }
         if constexpr (PREC == 1 && FLUX == FLUX_ROE && NV >= 4) roe_md_mixed<NV, AX>(fl, fr, fx);
+        else if constexpr (PREC == 1 && FLUX == FLUX_HLLC && NV >= 4) hllc_md_mixed<NV, AX>(fl, fr, fx);
         else riemann<NV, AX, FLUX>(fl, fr, fx);
         int fslot = fring(j - s_begin + FO);
 #pragma unroll

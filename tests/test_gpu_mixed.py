@@ -36,10 +36,12 @@ def vortex_l1(n, precision, t_end, im=11, fm=1):
 
 
 @pytest.mark.parametrize("n", [64, 128, 256])
-def test_mixed_vortex_error_within_2x_of_fp64(n):
+@pytest.mark.parametrize("im,fm", [(11, 1), (2, 0)])
+def test_mixed_vortex_error_within_2x_of_fp64(n, im, fm):
+    """TENO5 + Roe (the benchmark scheme) and WCNS5 + HLLC."""
     t_end = 0.5
-    e64 = vortex_l1(n, 0, t_end)
-    emx = vortex_l1(n, 1, t_end)
+    e64 = vortex_l1(n, 0, t_end, im, fm)
+    emx = vortex_l1(n, 1, t_end, im, fm)
     assert emx <= 2.0 * e64, (n, e64, emx)
 
 
