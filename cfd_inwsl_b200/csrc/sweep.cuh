@@ -125,7 +125,11 @@ struct SweepShape {
     static constexpr int RF = pow2_ceil(S + FC);     // face ring positions (S + FC used)
     static constexpr int LSP = R | 1;         // odd line strides avoid bank conflicts
     static constexpr int LSF = RF | 1;
-    static constexpr int SMEM_DOUBLES = 2 * NV * W * LSP + NV * W * LSF;
+    // The 3D mixed y/z sweeps keep no FP64 cons ring: they read the cons as
+    // hi + lo from the FP32 split (within 2^-48 of the cons), which leaves room
+    // for the cp.async staging below (the x sweep stages less and has room).
+    static constexpr bool HL_CS = (PREC == 1 && NV == 5 && AX != 0 && FAM != FAM_RESEARCH);
+    static constexpr int SMEM_DOUBLES = (HL_CS ? 1 : 2) * NV * W * LSP + NV * W * LSF;
     // mixed form: FP32 hi/lo split of the cons ring (exact FP32 increments)
     static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
     static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
@@ -161,8 +165,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     const double rkBdt = p.ctl ? p.ctl->bdt[p.rk_stage] : p.rkBdt;
     extern __shared__ double smem[];
     double *sp = smem;                   // [NV][W][LSP] prim
-    double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue)
-    double *sf = sc + NV * W * LSP;      // [NV][W][LSF] face flux
+    double *sc = sp + NV * W * LSP;      // [NV][W][LSP] cons re-derived from prim (primToChar prologue); absent with HL_CS
+    double *sf = SH::HL_CS ? sc : sc + NV * W * LSP;  // [NV][W][LSF] face flux
     // mixed form: [NV][W][LSP] (hi, lo) = ((float)cons, (float)(cons - hi))
     float2 *shl = reinterpret_cast<float2 *>(sf + NV * W * LSF);
     // staging: [0] next chunk's cons, [1] rhs, [2] U^0, [3] U^k; [NV][NT] each
@@ -227,7 +231,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             sp[(v * W + l) * LSP + slot] = pr[v];
-            sc[(v * W + l) * LSP + slot] = cs[v];
+            if constexpr (!SH::HL_CS) sc[(v * W + l) * LSP + slot] = cs[v];
             if constexpr (PREC == 1) {
                 const float hi = (float)cs[v];
                 shl[(v * W + l) * LSP + slot] = make_float2(hi, (float)(cs[v] - (double)hi));
@@ -262,7 +266,15 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 auto hlacc = [&](int m, int v) {
                     return hll[v * W * LSP + slot[m]];
                 };
-                reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, hlacc, p.icst, p.icst_k, fl, fr);
+                if constexpr (SH::HL_CS) {
+                    auto hlcs = [&](int m, int v) {
+                        const float2 t = hlacc(m, v);
+                        return (double)t.x + (double)t.y;
+                    };
+                    reconstruct_face_mixed<NV, AX, FAM>(hlcs, pracc, hlacc, p.icst, p.icst_k, fl, fr);
+                } else {
+                    reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, hlacc, p.icst, p.icst_k, fl, fr);
+                }
             } else {
                 reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, p.icst_k, fl, fr);
             }
@@ -571,9 +583,18 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
                                      : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, kYS, kYW>(p, st);
         }
         if constexpr (NV == 5) {
-            if (ax == 2)
+            if (ax == 2) {
+#if defined(CFD_FAST)
+                if constexpr (FAM != FAM_RESEARCH && CFD_MIXED_Z16) {
+                    if (p.prec == 1 && p.diff != DIFF_TRAD6)
+                        return flux == FLUX_HLLC
+                                   ? launch_sweep_shape_p<NV, 2, FAM, FLUX_HLLC, kYSm, kYWm, 1, 0>(p, st)
+                                   : launch_sweep_shape_p<NV, 2, FAM, FLUX_ROE, kYSm, kYWm, 1, 0>(p, st);
+                }
+#endif
                 return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, kYS, kYW>(p, st)
                                          : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, kYS, kYW>(p, st);
+            }
         }
         return cudaErrorInvalidValue;
     }

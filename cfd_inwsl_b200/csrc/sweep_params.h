@@ -29,6 +29,9 @@ constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
 #define CFD_YWM 16
 #endif
 constexpr int kYSm = CFD_YSM, kYWm = CFD_YWM;  // along y, mixed form (single grid)
+#ifndef CFD_MIXED_Z16
+#define CFD_MIXED_Z16 1  // the mixed form's z sweep takes the kYSm x kYWm shape too (0: kYS x kYW)
+#endif
 constexpr int k1S = 128, k1W = 1;          // 1D
 // Alternative shapes of the batched 2D/3D FP64 sweeps, picked per direction by
 // the batch autotuner: 32 threads per x line (8 lines per CTA), 16 threads per
