@@ -198,26 +198,42 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         base = (long long)a * p.stride[T0] + (long long)bb * p.stride[T1];
         lid = a + nt0 * bb;
     };
+    // the thread's own line, fixed for the whole tile: held in registers by
+    // the mixed form, recomputed where needed by the FP64 form (whose kernels
+    // have no registers to spare)
+    bool my_ok = false; long long my_base = 0; int my_lid = 0;
+    if constexpr (PREC == 1) line_of(tl, my_ok, my_base, my_lid);
+    auto own_line = [&](bool &ok, long long &base, int &lid) {
+        if constexpr (PREC == 1) {
+            ok = my_ok; base = my_base; lid = my_lid;
+        } else {
+            line_of(tl, ok, base, lid);
+        }
+    };
 
     // Stage cell P (global index along AX, may be a ghost) of line l; staged:
     // its cons already sit in stg[0] (interior cells of the thread's own line).
     auto load_pos = [&](int l, int P, bool staged = false) {
         bool ok; long long base; int lid;
-        line_of(l, ok, base, lid);
+        if (PREC == 1 && l == tl) own_line(ok, base, lid);
+        else line_of(l, ok, base, lid);
         double pr[NV];
+        double cs[NV];
+        bool have_cs = false;  // the mixed form takes interior cells' cons as loaded
         if (!ok) {
             pr[0] = 1.0;
             for (int v = 1; v < NV - 1; v++) pr[v] = 0.0;
             pr[NV - 1] = 1.0;
         } else if (P >= 0 && P < nd) {
             if (staged) {
-                double c[NV];
 #pragma unroll
-                for (int v = 0; v < NV; v++) c[v] = stg[v * NT + threadIdx.x];
-                cons_to_prim<NV>(c, pr);
+                for (int v = 0; v < NV; v++) cs[v] = stg[v * NT + threadIdx.x];
             } else {
-                load_cons_prim<NV>(p.u, p.ncell, base + (long long)P * sAX, pr);
+#pragma unroll
+                for (int v = 0; v < NV; v++) cs[v] = __ldg(p.u + v * p.ncell + base + (long long)P * sAX);
             }
+            cons_to_prim<NV>(cs, pr);
+            have_cs = (PREC == 1);
         } else if (P < 0) {
             int k = -P - 1;
             ghost_prim<NV, HG>(p, p.bc_lo[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
@@ -225,8 +241,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             int k = P - nd;
             ghost_prim<NV, HG>(p, p.bc_hi[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
         }
-        double cs[NV];
-        prim_to_cons<NV>(pr, cs);
+        if (!have_cs) prim_to_cons<NV>(pr, cs);  // as the reference's primToChar re-derives them
         int slot = ring(P - s_begin + HG);
 #pragma unroll
         for (int v = 0; v < NV; v++) {
@@ -300,7 +315,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     // cp.async of this thread's interior cell at position P into stg[0]
     auto prefetch_cell = [&](int P) {
         bool ok; long long base; int lid;
-        line_of(tl, ok, base, lid);
+        own_line(ok, base, lid);
         if (ok && P >= 0 && P < nd) {
             const long long cell = base + (long long)P * sAX;
 #pragma unroll
@@ -313,7 +328,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                need_u = PF_EPI && p.mode == MODE_RK && p.rk_stage != 1;
     auto prefetch_epilogue = [&](int i) {
         bool ok; long long base; int lid;
-        line_of(tl, ok, base, lid);
+        own_line(ok, base, lid);
         if (ok && i < s_end) {
             const long long cell = base + (long long)i * sAX;
 #pragma unroll
@@ -350,7 +365,7 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 
         const int i = c0 + tp;
         bool ok; long long base; int lid;
-        line_of(tl, ok, base, lid);
+        own_line(ok, base, lid);
         if constexpr (PF) __pipeline_wait_prior(1);  // the epilogue operands; the next cell may still fly
         if (ok && i < s_end) {
             double fnm[NV], fnp[NV];
