@@ -486,11 +486,20 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = None
+    fp64 = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
         t = json.loads(tp.read_text()).get(args.workload)
         if t:
             traffic = t.get("bytes_per_launch")
+            ops = t.get("fp64_ops_per_face")
+            if ops and args.precision == "fp64":
+                # the path's binding roof: FP64 arithmetic (counted instructions
+                # per face from ncu, times the faces of one launch, over the
+                # live kernel time), against B200's nominal FP64 vector peak
+                tflops = ops["flops"] * ncell / (kern_ms / 1e3) / 1e12
+                fp64 = {"achieved_tflops": tflops, "peak_tflops": 37.0, "peak_source": "nominal (B200 datasheet)",
+                        "frac": tflops / 37.0, "flops_per_face": ops["flops"], "count_source": ops["source"]}
 
     # ---- e2e through the C ABI with host buffers
     e2e_steps = max(2, min(args.steps // 10, 10))
@@ -579,7 +588,8 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": f"sweep along axis {dim - 1} with the RK stage epilogue",
                      "kernel_ms": kern_ms, "first_sweep_ms": kern0_ms,
                      "algorithmic_bytes_per_cell": bytes_per_cell,
-                     "note": "FP64-arithmetic bound path; the HBM fraction is low by construction"},
+                     "note": "FP64-arithmetic bound path; the HBM fraction is low by construction",
+                     "fp64": fp64},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes + 16, "steps": e2e_steps,
                 "path": ("cfd_upload_cons + one step (" + ("stages with halo exchanges" if slab is not None
