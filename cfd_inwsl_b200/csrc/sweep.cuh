@@ -104,6 +104,9 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
 #ifndef CFD_SWEEP_MINB
 #define CFD_SWEEP_MINB 2
 #endif
+#ifndef CFD_SWEEP_MINB128
+#define CFD_SWEEP_MINB128 4  // resident 128-thread CTAs per SM (2D/3D)
+#endif
 
 constexpr int pow2_ceil(int x)
 {
@@ -135,7 +138,14 @@ struct SweepShape {
     static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
     // Resident CTAs per SM the launch bounds ask for: 512 threads per SM in
     // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread.
-    static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? CFD_SWEEP_MINB * (256 / NT) : CFD_SWEEP_MINB) : 1;
+    // Three resident 128-thread CTAs (about 170 registers, fewer spills)
+    // measured faster for TENO-Z along x in FP64 and in every 3D mixed sweep;
+    // four for the others.
+    static constexpr bool THREE = (FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5);
+    static constexpr int MINB128 = THREE ? 3 : CFD_SWEEP_MINB128;
+    static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? (NT == 128 ? MINB128 : CFD_SWEEP_MINB * (256 / NT))
+                                                       : CFD_SWEEP_MINB)
+                                            : 1;
     // Asynchronous staging (cp.async) of each thread's global operands: the next
     // chunk's cell and the epilogue's rhs / U^0 / U^k, so that their latency
     // hides behind the face phase. Only where MINB CTAs per SM still fit in the
