@@ -11,13 +11,14 @@
 // and one segment [s_begin, s_end) of them. It marches through the segment in
 // chunks of S cells. Per chunk it
 //   1. loads the S new cells (cons -> prim on the fly, ghost cells from the
-//      line's boundary wiring) into a shared-memory ring of S+8 positions,
+//      line's boundary wiring) into a shared-memory ring of S+8 positions
+//      (S+10 with the TRAD6 difference),
 //   2. computes the S new face fluxes (one face per thread) into a ring of
-//      S+3 faces; the 3 faces shared with the previous chunk are reused,
+//      S+3 faces (S+5); the faces shared with the previous chunk are reused,
 //   3. applies the MND6 difference (node fluxes recomputed from the prim ring)
-//      and the epilogue for S cells.
+//      or the TRAD6 one, and the epilogue for S cells.
 // Face values and face fluxes never leave shared memory, and every cell is
-// read from HBM once per sweep plus 8 halo cells per line segment.
+// read from HBM once per sweep plus 8 (10) halo cells per line segment.
 //
 // Thread layout: along x (AX = 0) consecutive threads take consecutive cells
 // of a line; along y/z consecutive threads take neighbouring lines (adjacent
