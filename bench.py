@@ -420,8 +420,8 @@ def run_ours(args, rank, world, local_rank):
 
     def run(k):
         if slab is not None:
-            for _ in range(k):
-                slab.step(slab.max_dt(cfl))
+            _, taken = slab.run_device(k, cfl)
+            assert taken == k
             return
         _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, k, C.byref(tbuf), C.byref(nsteps), None, None), solver.h)
         assert nsteps.value == k
@@ -511,7 +511,7 @@ def run_ours(args, rank, world, local_rank):
     def e2e_step():
         _lib.check(lib.cfd_upload_cons(solver.h, hp), solver.h)
         if slab is not None:
-            slab.step(slab.max_dt(cfl))
+            slab.run_device(1, cfl)
         else:
             _lib.check(lib.cfd_run(solver.h, cfl, 1, 1e300, 1, C.byref(tbuf), C.byref(nsteps), _lib.ptr(dts),
                                    _lib.ptr(lin)), solver.h)

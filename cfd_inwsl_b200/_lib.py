@@ -96,6 +96,12 @@ _PROTOS = {
     "cfd_adjoint_reverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "cfd_enable_halo": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
     "cfd_stage_state": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cfd_loop_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "cfd_reduction_words": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cfd_loop_step_begin": (C.c_int, [C.c_void_p]),
+    "cfd_loop_stage": (C.c_int, [C.c_void_p, C.c_int]),
+    "cfd_loop_step_end": (C.c_int, [C.c_void_p]),
+    "cfd_loop_end": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "cfd_rk3_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
     "cfd_max_wave_speeds": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_save_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),

@@ -1850,6 +1850,74 @@ int cfd_max_wave_speeds(cfd_handle *h, double *lam)
     return CFD_OK;
 }
 
+int cfd_loop_begin(cfd_handle *h, double cfl, double t)
+{
+    if (!h || !(cfl > 0.0)) return CFD_ERR_CONFIG;
+    int rc;
+    if ((rc = sync_bc(h)) || (rc = ensure_run_buffers(h, 1))) return rc;
+    if (!h->ws_valid && (rc = launch_wave_speed(h))) return rc;
+    cfd::StepCtl *c = h->ctl_host;
+    std::memset(c, 0, sizeof(*c));
+    c->t = t;
+    c->outputDt = 1e300;  // no output clipping: every step takes dt = CFL / sum_d lambda_d
+    c->cfl = cfl;
+    c->endStep = 1;
+    c->maxSteps = 0x7fffffff;
+    CFD_CUDA(h, cudaMemcpyAsync(h->ctl, c, sizeof(*c), cudaMemcpyHostToDevice, h->stream));
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+    return CFD_OK;
+}
+
+int cfd_reduction_words(cfd_handle *h, unsigned long long **words)
+{
+    if (!h || !words) return CFD_ERR_CONFIG;
+    *words = h->red;
+    return CFD_OK;
+}
+
+int cfd_loop_step_begin(cfd_handle *h)
+{
+    if (!h || !h->ctl) return CFD_ERR_CONFIG;
+    step_begin_kernel<<<1, 1, 0, h->stream>>>(h->ctl, h->red, h->dim, nullptr);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    return CFD_OK;
+}
+
+int cfd_loop_stage(cfd_handle *h, int stage)
+{
+    if (!h || !h->ctl || stage < 1 || stage > 3) return CFD_ERR_CONFIG;
+    double *U0 = h->u[h->cur], *U1 = h->u[(h->cur + 1) % 3], *U2 = h->u[(h->cur + 2) % 3];
+    // dt and stage time come from the device step control (the coefficients
+    // of the host form, cfd_rk3_stage, with Bdt taken from ctl->bdt[stage])
+    if (stage == 1) return rk_stage(h, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
+    if (stage == 2) return rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl);
+    return rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl);
+}
+
+int cfd_loop_step_end(cfd_handle *h)
+{
+    if (!h || !h->ctl) return CFD_ERR_CONFIG;
+    step_end_kernel<<<1, 1, 0, h->stream>>>(h->ctl, h->red, nullptr);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    h->cur = (h->cur + 1) % 3;
+    h->ws_valid = true;  // stage 3 left this handle's wave speeds in the reduction words
+    return CFD_OK;
+}
+
+int cfd_loop_end(cfd_handle *h, double *t, int *nsteps)
+{
+    if (!h || !h->ctl) return CFD_ERR_CONFIG;
+    CFD_CUDA(h, cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(cfd::StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    unsigned err = 0;
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (t) *t = h->ctl_host->t;
+    if (nsteps) *nsteps = h->ctl_host->k;
+    return check_err(h, err);
+}
+
 // ------------------------------------------------------------------ checkpoint / restart
 
 namespace {

@@ -51,14 +51,14 @@ def neighbours(k: int, parts: int, periodic: bool) -> tuple[int | None, int | No
 class _DevArray:
     """A device buffer of this library seen by torch without a copy."""
 
-    def __init__(self, ptr: int, shape):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+    def __init__(self, ptr: int, shape, typestr: str = "<f8"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3, "strides": None}
 
 
-def _tensor(ptr: int, shape, device):
+def _tensor(ptr: int, shape, device, typestr: str = "<f8"):
     import torch
-    return torch.as_tensor(_DevArray(ptr, shape), device=device)
+    return torch.as_tensor(_DevArray(ptr, shape, typestr), device=device)
 
 
 class Slab:
@@ -107,6 +107,14 @@ class Slab:
 
     def set_stream(self, stream):
         _lib.check(self.lib.cfd_set_stream(self.solver.h, C.c_void_p(stream.cuda_stream)), self.solver.h)
+
+    def reduction_words(self):
+        """The 4 reduction words (max |R_rho|, wave speed per direction) as an
+        int64 device tensor: IEEE bit patterns of non-negative doubles, ordered
+        like the integers, so a MAX all-reduce gives the global maxima."""
+        ptr = C.c_void_p()
+        _lib.check(self.lib.cfd_reduction_words(self.solver.h, C.byref(ptr)), self.solver.h)
+        return _tensor(ptr.value, (4,), f"cuda:{self.device}", "<i8")
 
     def wave_speeds(self) -> np.ndarray:
         lam = np.zeros(3)
@@ -232,6 +240,28 @@ class SlabRank:
         for stage in (1, 2, 3):
             self.exchange(stage)
             self.slab.stage(stage, dt, t)
+
+    def run_device(self, steps: int, cfl: float, t: float = 0.0) -> tuple[float, int]:
+        """`steps` CFL steps with dt kept on the device: per step a MAX
+        all-reduce of the reduction words, then the three stages each after
+        its halo exchange, all enqueued on the slab's stream with no host
+        round trip (cfd_loop_*). Returns the end time and the steps taken."""
+        import torch
+        lib, h = self.slab.lib, self.slab.solver.h
+        with torch.cuda.stream(self.stream):
+            _lib.check(lib.cfd_loop_begin(h, float(cfl), float(t)), h)
+            words = self.slab.reduction_words()
+            for _ in range(steps):
+                self.dist.all_reduce(words, op=self.dist.ReduceOp.MAX, group=self.group)
+                _lib.check(lib.cfd_loop_step_begin(h), h)
+                for stage in (1, 2, 3):
+                    exchange_rows(self.dist, self.group, self.rank, self.nb, self.slab.stage_state(stage),
+                                  self.slab.halo)
+                    _lib.check(lib.cfd_loop_stage(h, stage), h)
+                _lib.check(lib.cfd_loop_step_end(h), h)
+            t_out, n = C.c_double(), C.c_int()
+            _lib.check(lib.cfd_loop_end(h, C.byref(t_out), C.byref(n)), h)
+        return t_out.value, n.value
 
 
 def exchange_rows(dist, group, rank, nb, state, halo):

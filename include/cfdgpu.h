@@ -301,6 +301,31 @@ int cfd_stage_state(cfd_handle *h, int stage, double **state);
 int cfd_rk3_stage(cfd_handle *h, int stage, double dt, double t);
 int cfd_max_wave_speeds(cfd_handle *h, double *lam);
 
+/* Device-controlled steps for callers that act between the stages (the slab
+ * decomposition: halo exchange before each stage, wave speeds reduced over
+ * ranks before each step) without a host round trip per step. No counterpart
+ * in the reference; one step is the sequence
+ *     [reduce the 4 words of cfd_reduction_words over ranks with MAX]
+ *     cfd_loop_step_begin; for stage 1..3: [halos], cfd_loop_stage; cfd_loop_step_end
+ * enqueued on the handle's stream, dt = CFL / sum_d lambda_d as
+ * getTimeIntervalExplicit (blockSolver.cpp:318-349) and the stage times of
+ * RK3_SSP kept on the device.
+ * cfd_loop_begin: starts at time t with the given CFL number (no output
+ *   clipping) and makes sure the reduction words hold the current state's wave
+ *   speeds.
+ * cfd_reduction_words: device pointer of 4 words: max |R_rho| of the last
+ *   step and the per-direction maximum wave speeds (c + |u_d|) / h_d, as the
+ *   IEEE bit patterns of non-negative doubles, whose order is that of the
+ *   64-bit integers: a MAX reduction over ranks as int64 gives the global ones.
+ * cfd_loop_end: waits for the stream and returns the time and the steps taken
+ *   since cfd_loop_begin (CFD_ERR_NONFINITE / NEGATIVE as cfd_rk3_step). */
+int cfd_loop_begin(cfd_handle *h, double cfl, double t);
+int cfd_reduction_words(cfd_handle *h, unsigned long long **words);
+int cfd_loop_step_begin(cfd_handle *h);
+int cfd_loop_stage(cfd_handle *h, int stage);
+int cfd_loop_step_end(cfd_handle *h);
+int cfd_loop_end(cfd_handle *h, double *t, int *nsteps);
+
 /* Binary checkpoint / restart of the state (the reference writes its output
  * through CGNS, cgnsio.cpp:3-101, and has no restart; libcgns is not part of
  * this library). Little-endian file: a 104-byte header (magic "CFDGPUCK",

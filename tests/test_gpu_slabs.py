@@ -2,10 +2,12 @@
 process, halos by device copies, against the undivided grid. The strict
 flavour must match bit for bit (every ghost is an exact copy of the
 neighbouring slab's cell); the fast flavour within 1e-13 relative."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
-from cfd_inwsl_b200 import slabs, zone
+from cfd_inwsl_b200 import _lib, slabs, zone
 from tests.util import make_info, quadrant_state, rel_linf, smooth_state_3d
 
 pytestmark = pytest.mark.gpu
@@ -99,6 +101,13 @@ def test_slab_rank_one_process_matches_whole_grid():
             assert rank.max_dt(info.CFL) == dt
             whole.RK3_SSP(dt)
             rank.step(dt)
+        np.testing.assert_array_equal(rank.slab.solver.cons, whole.cons)
+        # the device-controlled form (dt reduced and kept on the device)
+        # against the undivided grid's device loop
+        tw, nw = C.c_double(0.0), C.c_int(0)
+        _lib.check(whole.lib.cfd_run(whole.h, info.CFL, 1, 1e300, 6, C.byref(tw), C.byref(nw), None, None), whole.h)
+        tr, nr = rank.run_device(6, info.CFL)
+        assert nr == nw.value == 6 and tr == tw.value
         np.testing.assert_array_equal(rank.slab.solver.cons, whole.cons)
     finally:
         dist.destroy_process_group()
