@@ -56,8 +56,11 @@ WORKLOADS = {
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except (ValueError, KeyError, TypeError):
+            pass
     return 6650.0, "fallback"
 
 
