@@ -294,6 +294,13 @@ struct cfd_handle {
     double *adj_buf[4] = {nullptr, nullptr, nullptr, nullptr};  // lambda, w, w2, face scratch (24 states)
     double adj_dt = 0.0;
     int adj_nsteps = 0, adj_every = 0;
+    // captured adjoint segments: K forward steps from each state slot (record)
+    // and one full segment's recomputation and reverse sweep; valid for
+    // (adj_graph_K, adj_graph_dt)
+    cudaGraphExec_t adj_rec_graph[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t adj_rev_graph = nullptr;
+    int adj_graph_K = 0;
+    double adj_graph_dt = 0.0;
     // slab decomposition: halo rows of the last direction's low / high side
     double *halo[2] = {nullptr, nullptr};
 };
@@ -551,6 +558,32 @@ void drop_graphs(cfd_handle *h)
             if (h->graph[g][k]) cudaGraphExecDestroy(h->graph[g][k]);
             h->graph[g][k] = nullptr;
         }
+    for (int k = 0; k < 3; k++) {
+        if (h->adj_rec_graph[k]) cudaGraphExecDestroy(h->adj_rec_graph[k]);
+        h->adj_rec_graph[k] = nullptr;
+    }
+    if (h->adj_rev_graph) cudaGraphExecDestroy(h->adj_rev_graph);
+    h->adj_rev_graph = nullptr;
+    h->adj_graph_K = 0;
+}
+
+// Capture the work `enqueue` puts on the handle's stream into an executable
+// graph (the launch count is the graph's, not the capture's).
+template <class F>
+int capture_graph(cfd_handle *h, F &&enqueue, cudaGraphExec_t *exec)
+{
+    unsigned long long saved = h->launches;
+    cudaGraph_t g;
+    CFD_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue();
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = saved;
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    return CFD_OK;
 }
 
 constexpr int kGraphSteps[3] = {1, 3, 12};
@@ -1707,13 +1740,36 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
     if ((rc = adjoint_states(h, h->adj_ckpt, nck))) return rc;
     const size_t state = sizeof(double) * h->ncell * h->nv;
     CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
-    for (int s = 0; s < nsteps; s++) {
-        double *U0 = h->u[h->cur], *U1 = h->u[(h->cur + 1) % 3], *U2 = h->u[(h->cur + 2) % 3];
-        if (s % ckpt_every == 0)
-            CFD_CUDA(h, cudaMemcpyAsync(h->adj_ckpt[s / ckpt_every], U0, state, cudaMemcpyDeviceToDevice, h->stream));
-        double *S[3] = {U0, U1, U2};
-        if ((rc = adjoint_step(h, dt, S, U1))) return rc;
-        h->cur = (h->cur + 1) % 3;
+    if (h->adj_graph_K != ckpt_every || h->adj_graph_dt != dt) {
+        drop_graphs(h);
+        h->adj_graph_K = ckpt_every;
+        h->adj_graph_dt = dt;
+    }
+    const int K = ckpt_every;
+    // `cnt` steps from state slot `slot` (buffers by role)
+    auto steps_from = [&](int slot, int cnt) -> int {
+        for (int j = 0; j < cnt; j++) {
+            const int c = (slot + j) % 3;
+            double *S[3] = {h->u[c], h->u[(c + 1) % 3], h->u[(c + 2) % 3]};
+            int r = adjoint_step(h, dt, S, S[1]);
+            if (r) return r;
+        }
+        return CFD_OK;
+    };
+    for (int s0 = 0; s0 < nsteps; s0 += K) {
+        const int cnt = std::min(K, nsteps - s0);
+        CFD_CUDA(h, cudaMemcpyAsync(h->adj_ckpt[s0 / K], h->u[h->cur], state, cudaMemcpyDeviceToDevice, h->stream));
+        if (cnt == K) {  // a full segment: one graph per starting slot
+            const int slot = h->cur;
+            if (!h->adj_rec_graph[slot] &&
+                (rc = capture_graph(h, [&] { return steps_from(slot, K); }, &h->adj_rec_graph[slot])))
+                return rc;
+            CFD_CUDA(h, cudaGraphLaunch(h->adj_rec_graph[slot], h->stream));
+            h->launches += 3ULL * h->dim * K;
+        } else if ((rc = steps_from(h->cur, cnt))) {
+            return rc;
+        }
+        h->cur = (h->cur + cnt) % 3;
     }
     h->ws_valid = false;
     h->adj_dt = dt;
@@ -1739,32 +1795,50 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
     CFD_CUDA(h, cudaMemcpyAsync(h->stage, dJ_dUN_aos, state, cudaMemcpyHostToDevice, h->stream));
     if ((rc = launch_aos_to_soa(h, h->stage, lam))) return rc;
     const int nseg = (N + K - 1) / K;
-    for (int seg = nseg - 1; seg >= 0; seg--) {
-        const int s0 = seg * K, cnt = std::min(K, N - s0);
+    // one segment of cnt steps whose first state is in adj_stage[0]
+    auto segment = [&](int cnt) -> int {
+        int r;
         // recompute the segment, keeping every stage state
-        CFD_CUDA(h, cudaMemcpyAsync(h->adj_stage[0], h->adj_ckpt[seg], state, cudaMemcpyDeviceToDevice, h->stream));
         for (int j = 0; j < cnt; j++) {
             double *S[3] = {h->adj_stage[3 * j], h->adj_stage[3 * j + 1], h->adj_stage[3 * j + 2]};
-            if (j + 1 < cnt && (rc = adjoint_step(h, dt, S, h->adj_stage[3 * (j + 1)]))) return rc;
+            if (j + 1 < cnt && (r = adjoint_step(h, dt, S, h->adj_stage[3 * (j + 1)]))) return r;
             if (j + 1 == cnt) {
                 // the last step's stages only (its output is not needed)
-                if ((rc = rk_stage(h, 1, S[0], S[0], S[1], 1.0, dt, 0.0, 0.0, false))) return rc;
-                if ((rc = rk_stage(h, 2, S[1], S[0], S[2], 0.75, 0.25 * dt, 0.25, 0.0, false))) return rc;
+                if ((r = rk_stage(h, 1, S[0], S[0], S[1], 1.0, dt, 0.0, 0.0, false))) return r;
+                if ((r = rk_stage(h, 2, S[1], S[0], S[2], 0.75, 0.25 * dt, 0.25, 0.0, false))) return r;
             }
         }
         // reverse through the segment's steps:
         //   U1 = U0 - dt R(U0); U2 = 3/4 U0 + 1/4 (U1 - dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 - dt R(U2))
         for (int j = cnt - 1; j >= 0; j--) {
             double *U0 = h->adj_stage[3 * j], *U1 = h->adj_stage[3 * j + 1], *U2 = h->adj_stage[3 * j + 2];
-            if ((rc = rhs_vjp(h, U2, lam, w))) return rc;                 // w = J(U2)^T lam3
-            if ((rc = axpby(h, 2.0 / 3.0, lam, -2.0 / 3.0 * dt, w))) return rc;  // w = lam2
-            if ((rc = axpby(h, 0.0, lam, 1.0 / 3.0, lam))) return rc;     // lam = lam3 / 3
-            if ((rc = rhs_vjp(h, U1, w, w2))) return rc;                  // w2 = J(U1)^T lam2
-            if ((rc = axpby(h, 0.25, w, -0.25 * dt, w2))) return rc;      // w2 = lam1
-            if ((rc = axpby(h, 0.75, w, 1.0, lam))) return rc;            // lam += 3/4 lam2
-            if ((rc = rhs_vjp(h, U0, w2, w))) return rc;                  // w = J(U0)^T lam1
-            if ((rc = axpby(h, 1.0, w2, 1.0, lam))) return rc;            // lam += lam1
-            if ((rc = axpby(h, -dt, w, 1.0, lam))) return rc;             // lam -= dt w
+            if ((r = rhs_vjp(h, U2, lam, w))) return r;                 // w = J(U2)^T lam3
+            if ((r = axpby(h, 2.0 / 3.0, lam, -2.0 / 3.0 * dt, w))) return r;  // w = lam2
+            if ((r = axpby(h, 0.0, lam, 1.0 / 3.0, lam))) return r;     // lam = lam3 / 3
+            if ((r = rhs_vjp(h, U1, w, w2))) return r;                  // w2 = J(U1)^T lam2
+            if ((r = axpby(h, 0.25, w, -0.25 * dt, w2))) return r;      // w2 = lam1
+            if ((r = axpby(h, 0.75, w, 1.0, lam))) return r;            // lam += 3/4 lam2
+            if ((r = rhs_vjp(h, U0, w2, w))) return r;                  // w = J(U0)^T lam1
+            if ((r = axpby(h, 1.0, w2, 1.0, lam))) return r;            // lam += lam1
+            if ((r = axpby(h, -dt, w, 1.0, lam))) return r;             // lam -= dt w
+        }
+        return CFD_OK;
+    };
+    if (h->adj_graph_K != K || h->adj_graph_dt != dt) {
+        drop_graphs(h);
+        h->adj_graph_K = K;
+        h->adj_graph_dt = dt;
+    }
+    for (int seg = nseg - 1; seg >= 0; seg--) {
+        const int s0 = seg * K, cnt = std::min(K, N - s0);
+        CFD_CUDA(h, cudaMemcpyAsync(h->adj_stage[0], h->adj_ckpt[seg], state, cudaMemcpyDeviceToDevice, h->stream));
+        if (cnt == K) {  // full segments replay one captured graph
+            if (!h->adj_rev_graph && (rc = capture_graph(h, [&] { return segment(K); }, &h->adj_rev_graph)))
+                return rc;
+            CFD_CUDA(h, cudaGraphLaunch(h->adj_rev_graph, h->stream));
+            h->launches += (3ULL * h->dim + 18ULL) * K;
+        } else if ((rc = segment(cnt))) {
+            return rc;
         }
     }
     if ((rc = launch_soa_to_aos(h, lam, h->stage, 0))) return rc;
