@@ -142,7 +142,8 @@ struct SweepShape {
     // Three resident 128-thread CTAs (about 170 registers, fewer spills)
     // measured faster for TENO-Z along x in FP64 and in every 3D mixed sweep;
     // four for the others.
-    static constexpr bool THREE = (FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5);
+    static constexpr bool THREE = ((FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5)) ||
+                                  (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0);
     static constexpr int MINB128 = THREE ? 3 : CFD_SWEEP_MINB128;
     static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? (NT == 128 ? MINB128 : CFD_SWEEP_MINB * (256 / NT))
                                                        : CFD_SWEEP_MINB)
@@ -605,6 +606,11 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
                                              : launch_sweep_shape_p<NV, 1, FAM, FLUX_ROE, kYSm, kYWm, 1, 0>(p, st);
             }
 #endif
+            if constexpr (NV == 5 && CFD_FP64_3D_YZ16) {
+                if (p.prec == 0 && p.diff != DIFF_TRAD6)
+                    return flux == FLUX_HLLC ? launch_sweep_shape_p<NV, 1, FAM, FLUX_HLLC, kYSm, kYWm, 0, 0>(p, st)
+                                             : launch_sweep_shape_p<NV, 1, FAM, FLUX_ROE, kYSm, kYWm, 0, 0>(p, st);
+            }
             return flux == FLUX_HLLC ? launch_sweep_shape<NV, 1, FAM, FLUX_HLLC, kYS, kYW>(p, st)
                                      : launch_sweep_shape<NV, 1, FAM, FLUX_ROE, kYS, kYW>(p, st);
         }
@@ -618,6 +624,12 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
                                    : launch_sweep_shape_p<NV, 2, FAM, FLUX_ROE, kYSm, kYWm, 1, 0>(p, st);
                 }
 #endif
+                if constexpr (CFD_FP64_3D_YZ16) {
+                    if (p.prec == 0 && p.diff != DIFF_TRAD6)
+                        return flux == FLUX_HLLC
+                                   ? launch_sweep_shape_p<NV, 2, FAM, FLUX_HLLC, kYSm, kYWm, 0, 0>(p, st)
+                                   : launch_sweep_shape_p<NV, 2, FAM, FLUX_ROE, kYSm, kYWm, 0, 0>(p, st);
+                }
                 return flux == FLUX_HLLC ? launch_sweep_shape<NV, 2, FAM, FLUX_HLLC, kYS, kYW>(p, st)
                                          : launch_sweep_shape<NV, 2, FAM, FLUX_ROE, kYS, kYW>(p, st);
             }
