@@ -538,7 +538,8 @@ int default_seg_len(const cfd_handle *h, int d)
     int W = (h->dim == 1) ? cfd::k1W : (d == 0 ? cfd::kXW : cfd::kYW);
     const bool mixed_shape = (d == 1 || (d == 2 && CFD_MIXED_Z16)) && h->cfg.precision == CFD_PREC_MIXED && !h->strict &&
                              h->fam != cfd::FAM_RESEARCH;
-    const bool fp64_shape = CFD_FP64_3D_YZ16 && h->dim == 3 && d > 0 && h->cfg.precision == CFD_PREC_FP64;
+    const bool fp64_shape = h->cfg.precision == CFD_PREC_FP64 &&
+                            ((CFD_FP64_3D_YZ16 && h->dim == 3 && d > 0) || (CFD_FP64_2D_Y16 && h->dim == 2 && d == 1));
     if (h->dim > 1 && (mixed_shape || fp64_shape) && h->cfg.diff_method != CFD_DIFF_TRAD6) {
         S = cfd::kYSm;  // the mixed form's y sweep shape (launch_sweep)
         W = cfd::kYWm;

@@ -143,7 +143,8 @@ struct SweepShape {
     // measured faster for TENO-Z along x in FP64 and in every 3D mixed sweep;
     // four for the others.
     static constexpr bool THREE = ((FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5)) ||
-                                  (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0);
+                                  (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0) ||
+                                  (CFD_FP64_2D_Y16 && PREC == 0 && NV == 4 && AX == 1);
     static constexpr int MINB128 = THREE ? 3 : CFD_SWEEP_MINB128;
     static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? (NT == 128 ? MINB128 : CFD_SWEEP_MINB * (256 / NT))
                                                        : CFD_SWEEP_MINB)
@@ -606,7 +607,7 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
                                              : launch_sweep_shape_p<NV, 1, FAM, FLUX_ROE, kYSm, kYWm, 1, 0>(p, st);
             }
 #endif
-            if constexpr (NV == 5 && CFD_FP64_3D_YZ16) {
+            if constexpr ((NV == 5 && CFD_FP64_3D_YZ16) || (NV == 4 && CFD_FP64_2D_Y16)) {
                 if (p.prec == 0 && p.diff != DIFF_TRAD6)
                     return flux == FLUX_HLLC ? launch_sweep_shape_p<NV, 1, FAM, FLUX_HLLC, kYSm, kYWm, 0, 0>(p, st)
                                              : launch_sweep_shape_p<NV, 1, FAM, FLUX_ROE, kYSm, kYWm, 0, 0>(p, st);

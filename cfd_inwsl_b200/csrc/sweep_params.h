@@ -6,9 +6,8 @@ namespace cfd {
 
 // Tile shapes of the sweeps: cells per chunk (S) x lines per CTA (W). CTAs of
 // 128 threads run three or four per SM (barriers across 4 warps instead of 8):
-// the x sweeps, the mixed form's y and z sweeps and the 3D FP64 y and z sweeps
-// take them; the 2D FP64 y sweep keeps 32 lines (256 threads), which measured
-// faster there.
+// every 2D/3D sweep takes them; the 32-line shapes (256 threads) remain for
+// the batched kernel and the TRAD6 difference.
 #ifndef CFD_XS
 #define CFD_XS 32
 #endif
@@ -32,6 +31,9 @@ constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
 constexpr int kYSm = CFD_YSM, kYWm = CFD_YWM;  // along y, mixed form (single grid)
 #ifndef CFD_FP64_3D_YZ16
 #define CFD_FP64_3D_YZ16 1  // the FP64 3D y/z sweeps take the kYSm x kYWm shape too (0: kYS x kYW)
+#endif
+#ifndef CFD_FP64_2D_Y16
+#define CFD_FP64_2D_Y16 1  // the FP64 2D y sweep takes the kYSm x kYWm shape too (0: kYS x kYW)
 #endif
 #ifndef CFD_MIXED_Z16
 #define CFD_MIXED_Z16 1  // the mixed form's z sweep takes the kYSm x kYWm shape too (0: kYS x kYW)
