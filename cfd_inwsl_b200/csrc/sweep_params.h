@@ -40,10 +40,10 @@ constexpr int kYSm = CFD_YSM, kYWm = CFD_YWM;  // along y, mixed form (single gr
 #endif
 constexpr int k1S = 128, k1W = 1;          // 1D
 // Alternative shapes of the batched 2D/3D FP64 sweeps, picked per direction by
-// the batch autotuner: 32 threads per x line (8 lines per CTA), 16 threads per
-// y/z line (16 lines per CTA).
+// the batch autotuner: 32 threads per x line (8 lines per CTA), 8 threads per
+// y/z line (16 lines per CTA, the single-grid FP64 shape).
 constexpr int kXS2 = 32, kXW2 = 8;
-constexpr int kYS2 = 16, kYW2 = 16;
+constexpr int kYS2 = 8, kYW2 = 16;
 
 
 // BndType values (zone_FD/src/include/macro.hpp:33-34) plus the 3D mirror.

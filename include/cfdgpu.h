@@ -237,9 +237,10 @@ int cfd_batch_run(cfd_batch *b, double cfl, int end_step, const double *output_d
 
 /* Autotuner of the batched sweeps (no counterpart in the reference). For each
  * direction it times the persistent first-stage sweep of the whole batch over
- * the tilings it can run: tile shape (0: the single-grid shape, 1: 32 threads
- * per x line / 16 per y and z line, 2D and 3D FP64 only), lines cut into 1 or
- * 2 segments, and one or as many persistent CTAs per SM as fit; keeps the
+ * the tilings it can run: tile shape in cells per chunk x lines per CTA
+ * (0: 32 x 4 along x, 8 x 32 along y and z; 1: 32 x 8 along x, 8 x 16 along
+ * y and z, 2D and 3D FP64 only), lines cut into 1 or 2 segments, and one or
+ * as many persistent CTAs per SM as fit; keeps the
  * fastest. Results are bit for bit those of any other tiling. The tuning runs
  * sweeps on the cases' current states and touches only scratch buffers (RHS,
  * stage state); call it between runs. choice (may be NULL) receives per
