@@ -547,7 +547,7 @@ int default_seg_len(const cfd_handle *h, int d)
     int t0, t1;
     transverse_axes(d, t0, t1);
     long long blocks_per_seg = (long long)((h->cfg.n[t0] + W - 1) / W) * h->cfg.n[t1];
-    const long long target = 148LL * 2 * 6;  // about six waves of two CTAs per SM
+    const long long target = 148LL * 2 * 6;  // about 1,800 CTAs: 3 to 6 waves at 2 to 4 resident per SM
     int seg = n;
     while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
     return seg;
