@@ -547,7 +547,10 @@ int default_seg_len(const cfd_handle *h, int d)
     int t0, t1;
     transverse_axes(d, t0, t1);
     long long blocks_per_seg = (long long)((h->cfg.n[t0] + W - 1) / W) * h->cfg.n[t1];
-    const long long target = 148LL * 2 * 6;  // about 1,800 CTAs: 3 to 6 waves at 2 to 4 resident per SM
+    // about 1,800 CTAs (3 to 6 waves at 2 to 4 resident per SM); the mixed
+    // form's x sweep measured fastest with half as many, longer segments
+    const bool mixed_x = d == 0 && h->dim > 1 && h->cfg.precision == CFD_PREC_MIXED;
+    const long long target = mixed_x ? 148LL * 2 * 3 : 148LL * 2 * 6;
     int seg = n;
     while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
     return seg;
