@@ -138,10 +138,10 @@ struct SweepShape {
     static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
     static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
     // Resident CTAs per SM the launch bounds ask for: 512 threads per SM in
-    // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread.
-    // Three resident 128-thread CTAs (about 170 registers, fewer spills)
-    // measured faster for TENO-Z along x in FP64 and in every 3D mixed sweep;
-    // four for the others.
+    // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread;
+    // or three 128-thread CTAs (168 registers, fewer spills), which measured
+    // faster for the FP64 y sweep (2D), the FP64 y and z sweeps (3D), the
+    // FP64 TENO-Z x sweep and the 3D mixed TENO-Z sweeps.
     static constexpr bool THREE = ((FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5)) ||
                                   (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0) ||
                                   (CFD_FP64_2D_Y16 && PREC == 0 && NV == 4 && AX == 1);
@@ -586,8 +586,9 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
     return cudaErrorInvalidValue;
 }
 
-// Tile shapes (kXS x kXW along x, kYS x kYW along y/z, kYSm x kYWm for the
-// mixed form along y, k1S x k1W in 1D): see sweep_params.h.
+// Tile shapes (sweep_params.h): kXS x kXW along x; kYSm x kYWm along y and z
+// for the single-grid sweeps; kYS x kYW along y and z for the TRAD6
+// difference and the batched kernel's default; k1S x k1W in 1D.
 template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st)
 {
