@@ -536,6 +536,11 @@ int default_seg_len(const cfd_handle *h, int d)
     int n = h->cfg.n[d];
     int S = (h->dim == 1) ? cfd::k1S : (d == 0 ? cfd::kXS : cfd::kYS);
     int W = (h->dim == 1) ? cfd::k1W : (d == 0 ? cfd::kXW : cfd::kYW);
+    if (h->dim > 1 && d == 0 && h->cfg.diff_method != CFD_DIFF_TRAD6 &&
+        (h->dim == 3 || h->cfg.precision == CFD_PREC_FP64)) {
+        S = cfd::kXSn;  // the x sweep shape of launch_sweep
+        W = cfd::kXWn;
+    }
     const bool mixed_shape = (d == 1 || (d == 2 && CFD_MIXED_Z16)) && h->cfg.precision == CFD_PREC_MIXED && !h->strict &&
                              h->fam != cfd::FAM_RESEARCH;
     const bool fp64_shape = h->cfg.precision == CFD_PREC_FP64 &&

@@ -586,9 +586,10 @@ static cudaError_t launch_sweep_shape(const SweepParams &p, cudaStream_t st)
     return cudaErrorInvalidValue;
 }
 
-// Tile shapes (sweep_params.h): kXS x kXW along x; kYSm x kYWm along y and z
-// for the single-grid sweeps; kYS x kYW along y and z for the TRAD6
-// difference and the batched kernel's default; k1S x k1W in 1D.
+// Tile shapes (sweep_params.h): kXSn x kXWn along x in 3D and for 2D FP64,
+// kXS x kXW along x for the 2D mixed form; kYSm x kYWm along y and z for the
+// single-grid sweeps; kXS x kXW and kYS x kYW for the TRAD6 difference and the
+// batched kernel's default; k1S x k1W in 1D.
 template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st)
 {
@@ -597,9 +598,14 @@ cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st
         return flux == FLUX_HLLC ? launch_sweep_shape<3, 0, FAM, FLUX_HLLC, k1S, k1W>(p, st)
                                  : launch_sweep_shape<3, 0, FAM, FLUX_ROE, k1S, k1W>(p, st);
     } else {
-        if (ax == 0)
+        if (ax == 0) {
+            // 16-cell chunks of 8 lines: faster in 3D (both forms) and for 2D FP64
+            if (p.diff != DIFF_TRAD6 && (NV == 5 || p.prec == 0))
+                return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, kXSn, kXWn>(p, st)
+                                         : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, kXSn, kXWn>(p, st);
             return flux == FLUX_HLLC ? launch_sweep_shape<NV, 0, FAM, FLUX_HLLC, kXS, kXW>(p, st)
                                      : launch_sweep_shape<NV, 0, FAM, FLUX_ROE, kXS, kXW>(p, st);
+        }
         if (ax == 1) {
 #if defined(CFD_FAST)
             if constexpr (FAM != FAM_RESEARCH) {

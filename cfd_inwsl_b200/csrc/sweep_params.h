@@ -20,7 +20,8 @@ namespace cfd {
 #ifndef CFD_YW
 #define CFD_YW 32
 #endif
-constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D/3D)
+constexpr int kXS = CFD_XS, kXW = CFD_XW;  // along x (2D mixed, TRAD6, batched default)
+constexpr int kXSn = 16, kXWn = 8;          // along x: 3D, and 2D FP64 (single grid)
 constexpr int kYS = CFD_YS, kYW = CFD_YW;  // along y and z
 #ifndef CFD_YSM
 #define CFD_YSM 8
