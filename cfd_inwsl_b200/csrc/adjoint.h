@@ -10,12 +10,12 @@
 namespace cfd {
 namespace adj {
 
-// One direction's share of lam = (dR/dU)^T mu, all arrays planar SoA
-// [4][nx*ny]. fam: interpolation family (0 WCNS5, 2 TENO-Z, 3 TENO-Cong) with
-// constant ct. P is scratch of 24 * nx * ny doubles (per-face contributions).
-// accumulate = false overwrites lam, true adds to it.
-cudaError_t launch_sweep_vjp(int axis, int fam, double ct, const double *u, const double *mu, double *lam, double *P,
-                             int nx, int ny, double h, bool accumulate, cudaStream_t st);
+// lam = (dR/dU)^T mu, all arrays planar SoA [4][nx*ny]. fam: interpolation
+// family (0 WCNS5, 2 TENO-Z, 3 TENO-Cong) with constant ct; hx, hy the
+// spacings of the x and y differences. P is scratch of 48 * nx * ny doubles
+// (per-face contributions of both directions).
+cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, double *lam, double *P, int nx,
+                           int ny, double hx, double hy, cudaStream_t st);
 
 // y = a * x + b * y over n doubles
 cudaError_t launch_axpby(double a, const double *x, double b, double *y, long long n, cudaStream_t st);

@@ -296,45 +296,72 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
     Rb[0] += rrb; Rb[1] += vrb[0]; Rb[2] += vrb[1]; Rb[3] += prb;
 }
 
-// Forward face flux of stencil U[6][4] and Ub += (dF/dU)^T Fb; interpolation
-// family fam (AdjInterp) with constant ct.
+// Roe average of a face stencil's cells 2 and 3, the eigenvectors (rows of
+// L, columns of R) and what they are built from (eigenSystem.cpp:13-86)
 template <int AX>
-ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][4], int fam = ADJ_WCNS5,
-                     double ct = 0.0)
-{
-    constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
-    double P2[4], P3[4];
-    c2p(U[2], P2);
-    c2p(U[3], P3);
-    // Roe average of cells 2 and 3 and the eigenvectors (eigenSystem.cpp:13-86)
-    const double s1 = sqrt(P2[0]), s2 = sqrt(P3[0]), iA = 1.0 / (s1 + s2);
-    const double HL = 0.5 * (P2[1] * P2[1] + P2[2] * P2[2]) + kGG1 * P2[3] / P2[0];
-    const double HR = 0.5 * (P3[1] * P3[1] + P3[2] * P3[2]) + kGG1 * P3[3] / P3[0];
-    const double u = (s1 * P2[1] + s2 * P3[1]) * iA, v = (s1 * P2[2] + s2 * P3[2]) * iA;
-    const double ht = (s1 * HL + s2 * HR) * iA;
-    const double ek = 0.5 * (u * u + v * v), h = ht - ek;
-    const double c = sqrt(kGm1 * h), ic = 1.0 / c, ih = 1.0 / h, Vn = nx * u + ny * v;
-    double L[4][4], R[4][4];
-    L[0][0] = -ny * u + nx * v; L[0][1] = ny; L[0][2] = -nx; L[0][3] = 0.0;
-    L[1][0] = h - ek; L[1][1] = u; L[1][2] = v; L[1][3] = -1.0;
-    L[2][0] = 0.5 * (Vn * ic + ek * ih); L[2][1] = 0.5 * (-nx * ic - u * ih); L[2][2] = 0.5 * (-ny * ic - v * ih);
-    L[2][3] = 0.5 * ih;
-    L[3][0] = 0.5 * (-Vn * ic + ek * ih); L[3][1] = 0.5 * (nx * ic - u * ih); L[3][2] = 0.5 * (ny * ic - v * ih);
-    L[3][3] = 0.5 * ih;
-    R[0][0] = 0.0; R[1][0] = ny; R[2][0] = -nx; R[3][0] = ny * u - nx * v;
-    R[0][1] = ih; R[1][1] = u * ih; R[2][1] = v * ih; R[3][1] = ek * ih;
-    R[0][2] = 1.0; R[1][2] = u - nx * c; R[2][2] = v - ny * c; R[3][2] = h + ek - Vn * c;
-    R[0][3] = 1.0; R[1][3] = u + nx * c; R[2][3] = v + ny * c; R[3][3] = h + ek + Vn * c;
+struct FaceEig {
+    double P2[4], P3[4], s1, s2, iA, HL, HR, u, v, ht, ek, h, c, ic, ih, Vn, L[4][4], R[4][4];
+    ADJ_HD explicit FaceEig(const double (&U)[6][4])
+    {
+        constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
+        c2p(U[2], P2);
+        c2p(U[3], P3);
+        s1 = sqrt(P2[0]); s2 = sqrt(P3[0]); iA = 1.0 / (s1 + s2);
+        HL = 0.5 * (P2[1] * P2[1] + P2[2] * P2[2]) + kGG1 * P2[3] / P2[0];
+        HR = 0.5 * (P3[1] * P3[1] + P3[2] * P3[2]) + kGG1 * P3[3] / P3[0];
+        u = (s1 * P2[1] + s2 * P3[1]) * iA; v = (s1 * P2[2] + s2 * P3[2]) * iA;
+        ht = (s1 * HL + s2 * HR) * iA;
+        ek = 0.5 * (u * u + v * v); h = ht - ek;
+        c = sqrt(kGm1 * h); ic = 1.0 / c; ih = 1.0 / h; Vn = nx * u + ny * v;
+        L[0][0] = -ny * u + nx * v; L[0][1] = ny; L[0][2] = -nx; L[0][3] = 0.0;
+        L[1][0] = h - ek; L[1][1] = u; L[1][2] = v; L[1][3] = -1.0;
+        L[2][0] = 0.5 * (Vn * ic + ek * ih); L[2][1] = 0.5 * (-nx * ic - u * ih); L[2][2] = 0.5 * (-ny * ic - v * ih);
+        L[2][3] = 0.5 * ih;
+        L[3][0] = 0.5 * (-Vn * ic + ek * ih); L[3][1] = 0.5 * (nx * ic - u * ih); L[3][2] = 0.5 * (ny * ic - v * ih);
+        L[3][3] = 0.5 * ih;
+        R[0][0] = 0.0; R[1][0] = ny; R[2][0] = -nx; R[3][0] = ny * u - nx * v;
+        R[0][1] = ih; R[1][1] = u * ih; R[2][1] = v * ih; R[3][1] = ek * ih;
+        R[0][2] = 1.0; R[1][2] = u - nx * c; R[2][2] = v - ny * c; R[3][2] = h + ek - Vn * c;
+        R[0][3] = 1.0; R[1][3] = u + nx * c; R[2][3] = v + ny * c; R[3][3] = h + ek + Vn * c;
+    }
+};
 
-    double q[4][6], QL[4], QR[4];
+// What the first half of a face adjoint hands the second: the interpolated
+// characteristic states with their TENO flags and the adjoints of the face's
+// reconstructed cons (clb, crb) and of the prims of cells 2 and 3 that the
+// positivity fallback used (P2b, P3b).
+struct FaceStates {
+    double QL[4], QR[4], clb[4], crb[4], P2b[4], P3b[4];
     unsigned flL[4], flR[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
+};
+
+// First half of the face adjoint: the forward to the face states and the
+// Roe flux's adjoint back to the reconstructed cons.
+template <int AX>
+ADJ_HD void face_vjp_states(const double (&U)[6][4], const double *Fb, FaceStates &f, int fam, double ct)
+{
+    const FaceEig<AX> e(U);
+    const double(&P2)[4] = e.P2;
+    const double(&P3)[4] = e.P3;
+    const double(&L)[4][4] = e.L;
+    const double(&R)[4][4] = e.R;
+    // characteristic values of field k on the six cells (recomputed in the
+    // reverse pass rather than kept: the stencil state is register-bound)
+    auto char_field = [&](int k, double *q) {
 #pragma unroll
         for (int j = 0; j < 6; j++)
-            q[k][j] = L[k][0] * U[j][0] + L[k][1] * U[j][1] + L[k][2] * U[j][2] + L[k][3] * U[j][3];
-        const double qm[5] = {q[k][5], q[k][4], q[k][3], q[k][2], q[k][1]};
-        QL[k] = interp5(fam, q[k], ct, flL[k]);
+            q[j] = L[k][0] * U[j][0] + L[k][1] * U[j][1] + L[k][2] * U[j][2] + L[k][3] * U[j][3];
+    };
+    double(&QL)[4] = f.QL;
+    double(&QR)[4] = f.QR;
+    unsigned(&flL)[4] = f.flL;
+    unsigned(&flR)[4] = f.flR;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double q[6];
+        char_field(k, q);
+        const double qm[5] = {q[5], q[4], q[3], q[2], q[1]};
+        QL[k] = interp5(fam, q, ct, flL[k]);
         QR[k] = interp5(fam, qm, ct, flR[k]);
     }
     double cl[4], cr[4], fl[4], fr[4];
@@ -356,7 +383,12 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
     // ---- reverse
     double flb[4] = {0, 0, 0, 0}, frb[4] = {0, 0, 0, 0};
     roe_vjp<AX>(fl, fr, Fb, flb, frb);
-    double P2b[4] = {0, 0, 0, 0}, P3b[4] = {0, 0, 0, 0}, clb[4] = {0, 0, 0, 0}, crb[4] = {0, 0, 0, 0};
+    double(&P2b)[4] = f.P2b;
+    double(&P3b)[4] = f.P3b;
+    double(&clb)[4] = f.clb;
+    double(&crb)[4] = f.crb;
+#pragma unroll
+    for (int i = 0; i < 4; i++) P2b[i] = P3b[i] = clb[i] = crb[i] = 0.0;
     if (fbl) {
         for (int i = 0; i < 4; i++) P2b[i] += flb[i];
     } else {
@@ -367,19 +399,57 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
     } else {
         c2p_adj(cr, fr, frb, crb);
     }
-    double Rb[4][4], Lb[4][4];
+}
+
+// Second half: the characteristic projections, the interpolations and the
+// eigensystem run backwards (the eigensystem is recomputed from U). Ub += .
+template <int AX>
+ADJ_HD void face_vjp_chars(const double (&U)[6][4], const FaceStates &f, double (&Ub)[6][4], int fam)
+{
+    constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
+    const FaceEig<AX> e(U);
+    const double(&P2)[4] = e.P2;
+    const double(&P3)[4] = e.P3;
+    const double(&L)[4][4] = e.L;
+    const double(&R)[4][4] = e.R;
+    const double s1 = e.s1, s2 = e.s2, iA = e.iA, HL = e.HL, HR = e.HR, u = e.u, v = e.v, ht = e.ht, ek = e.ek,
+                 h = e.h, c = e.c, ic = e.ic, ih = e.ih, Vn = e.Vn;
+    (void)h;
+    // characteristic values of field k on the six cells (recomputed in the
+    // reverse pass rather than kept: the stencil state is register-bound)
+    auto char_field = [&](int k, double *q) {
+#pragma unroll
+        for (int j = 0; j < 6; j++)
+            q[j] = L[k][0] * U[j][0] + L[k][1] * U[j][1] + L[k][2] * U[j][2] + L[k][3] * U[j][3];
+    };
+    const double(&QL)[4] = f.QL;
+    const double(&QR)[4] = f.QR;
+    const double(&clb)[4] = f.clb;
+    const double(&crb)[4] = f.crb;
+    const unsigned(&flL)[4] = f.flL;
+    const unsigned(&flR)[4] = f.flR;
+    double P2b[4], P3b[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        P2b[i] = f.P2b[i];
+        P3b[i] = f.P3b[i];
+    }
+    // eigenvector entries -> (u, v, h, c, ek, Vn, 1/c, 1/h); each row of L's
+    // adjoint goes into these as soon as it is formed
+    double ub = 0, vb = 0, hb = 0, cb = 0, ekb = 0, Vnb = 0, icb = 0, ihb = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const double QLb = R[0][k] * clb[0] + R[1][k] * clb[1] + R[2][k] * clb[2] + R[3][k] * clb[3];
         const double QRb = R[0][k] * crb[0] + R[1][k] * crb[1] + R[2][k] * crb[2] + R[3][k] * crb[3];
-#pragma unroll
-        for (int i = 0; i < 4; i++) Rb[i][k] = QL[k] * clb[i] + QR[k] * crb[i];
+        double q[6];
+        char_field(k, q);
         double qb[6] = {0, 0, 0, 0, 0, 0};
-        interp5_adj(fam, q[k], flL[k], QLb, qb);
-        const double qm[5] = {q[k][5], q[k][4], q[k][3], q[k][2], q[k][1]};
+        interp5_adj(fam, q, flL[k], QLb, qb);
+        const double qm[5] = {q[5], q[4], q[3], q[2], q[1]};
         double qmb[5] = {0, 0, 0, 0, 0};
         interp5_adj(fam, qm, flR[k], QRb, qmb);
         qb[5] += qmb[0]; qb[4] += qmb[1]; qb[3] += qmb[2]; qb[2] += qmb[3]; qb[1] += qmb[4];
+        double Lb[4];
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             double lb = 0.0;
@@ -388,34 +458,30 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
                 Ub[j][m] += L[k][m] * qb[j];
                 lb += qb[j] * U[j][m];
             }
-            Lb[k][m] = lb;
+            Lb[m] = lb;
+        }
+        if (k == 0) {
+            ub += -ny * Lb[0]; vb += nx * Lb[0];
+        } else if (k == 1) {
+            hb += Lb[0]; ekb -= Lb[0]; ub += Lb[1]; vb += Lb[2];
+        } else {  // rows 2 and 3 differ in the sign of their 1/c terms
+            const double sg = (k == 2) ? 1.0 : -1.0;
+            const double g0 = 0.5 * Lb[0], g1 = 0.5 * Lb[1], g2 = 0.5 * Lb[2], g3 = 0.5 * Lb[3];
+            Vnb += sg * ic * g0; icb += sg * Vn * g0; ekb += ih * g0; ihb += ek * g0;
+            icb -= sg * nx * g1; ub -= ih * g1; ihb -= u * g1;
+            icb -= sg * ny * g2; vb -= ih * g2; ihb -= v * g2;
+            ihb += g3;
         }
     }
-    // eigenvector entries -> (u, v, h, c, ek, Vn, 1/c, 1/h)
-    double ub = 0, vb = 0, hb = 0, cb = 0, ekb = 0, Vnb = 0, icb = 0, ihb = 0;
-    ub += -ny * Lb[0][0]; vb += nx * Lb[0][0];
-    hb += Lb[1][0]; ekb -= Lb[1][0]; ub += Lb[1][1]; vb += Lb[1][2];
-    {
-        const double g0 = 0.5 * Lb[2][0], g1 = 0.5 * Lb[2][1], g2 = 0.5 * Lb[2][2], g3 = 0.5 * Lb[2][3];
-        Vnb += ic * g0; icb += Vn * g0; ekb += ih * g0; ihb += ek * g0;
-        icb -= nx * g1; ub -= ih * g1; ihb -= u * g1;
-        icb -= ny * g2; vb -= ih * g2; ihb -= v * g2;
-        ihb += g3;
-    }
-    {
-        const double g0 = 0.5 * Lb[3][0], g1 = 0.5 * Lb[3][1], g2 = 0.5 * Lb[3][2], g3 = 0.5 * Lb[3][3];
-        Vnb -= ic * g0; icb -= Vn * g0; ekb += ih * g0; ihb += ek * g0;
-        icb += nx * g1; ub -= ih * g1; ihb -= u * g1;
-        icb += ny * g2; vb -= ih * g2; ihb -= v * g2;
-        ihb += g3;
-    }
-    ub += ny * Rb[3][0]; vb -= nx * Rb[3][0];
-    ihb += Rb[0][1] + u * Rb[1][1] + v * Rb[2][1] + ek * Rb[3][1];
-    ub += ih * Rb[1][1]; vb += ih * Rb[2][1]; ekb += ih * Rb[3][1];
-    ub += Rb[1][2]; cb -= nx * Rb[1][2]; vb += Rb[2][2]; cb -= ny * Rb[2][2];
-    hb += Rb[3][2]; ekb += Rb[3][2]; Vnb -= c * Rb[3][2]; cb -= Vn * Rb[3][2];
-    ub += Rb[1][3]; cb += nx * Rb[1][3]; vb += Rb[2][3]; cb += ny * Rb[2][3];
-    hb += Rb[3][3]; ekb += Rb[3][3]; Vnb += c * Rb[3][3]; cb += Vn * Rb[3][3];
+    // adjoint of R entry (i, k)
+    auto Rb = [&](int i, int k) { return QL[k] * clb[i] + QR[k] * crb[i]; };
+    ub += ny * Rb(3, 0); vb -= nx * Rb(3, 0);
+    ihb += Rb(0, 1) + u * Rb(1, 1) + v * Rb(2, 1) + ek * Rb(3, 1);
+    ub += ih * Rb(1, 1); vb += ih * Rb(2, 1); ekb += ih * Rb(3, 1);
+    ub += Rb(1, 2); cb -= nx * Rb(1, 2); vb += Rb(2, 2); cb -= ny * Rb(2, 2);
+    hb += Rb(3, 2); ekb += Rb(3, 2); Vnb -= c * Rb(3, 2); cb -= Vn * Rb(3, 2);
+    ub += Rb(1, 3); cb += nx * Rb(1, 3); vb += Rb(2, 3); cb += ny * Rb(2, 3);
+    hb += Rb(3, 3); ekb += Rb(3, 3); Vnb += c * Rb(3, 3); cb += Vn * Rb(3, 3);
     cb -= ic * ic * icb;
     hb -= ih * ih * ihb;
     hb += cb * kGm1 * 0.5 * ic;
@@ -434,6 +500,17 @@ ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][
     P3b[0] += -kGG1 * P3[3] / (P3[0] * P3[0]) * HRb + s2b * 0.5 / s2;
     c2p_adj(U[2], P2, P2b, Ub[2]);
     c2p_adj(U[3], P3, P3b, Ub[3]);
+}
+
+// Forward face flux of stencil U[6][4] and Ub += (dF/dU)^T Fb; interpolation
+// family fam (AdjInterp) with constant ct.
+template <int AX>
+ADJ_HD void face_vjp(const double (&U)[6][4], const double *Fb, double (&Ub)[6][4], int fam = ADJ_WCNS5,
+                     double ct = 0.0)
+{
+    FaceStates f;
+    face_vjp_states<AX>(U, Fb, f, fam, ct);
+    face_vjp_chars<AX>(U, f, Ub, fam);
 }
 
 // node flux (fluxSolveEuler2D) adjoint w.r.t. the cell's cons: cb += (dG/dU)^T Gb

@@ -1666,7 +1666,7 @@ int adjoint_buffers(cfd_handle *h)
     const size_t state = sizeof(double) * h->ncell * h->nv;
     for (int k = 0; k < 4; k++) {
         if (h->adj_buf[k]) continue;
-        cudaError_t e = cudaMalloc(&h->adj_buf[k], k == 3 ? 6 * state : state);
+        cudaError_t e = cudaMalloc(&h->adj_buf[k], k == 3 ? 12 * state : state);
         if (e != cudaSuccess) {
             h->adj_buf[k] = nullptr;
             return fail(h, CFD_ERR_NOMEM, "adjoint work buffers");
@@ -1679,12 +1679,10 @@ int adjoint_buffers(cfd_handle *h)
 int rhs_vjp(cfd_handle *h, const double *U, const double *mu, double *w)
 {
     const int nx = h->cfg.n[0], ny = h->cfg.n[1];
-    for (int d = 0; d < 2; d++) {
-        cudaError_t e = cfd::adj::launch_sweep_vjp(d, h->fam, h->icst, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[d],
-                                                   d > 0, h->stream);
-        if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
-        h->launches += 2;
-    }
+    cudaError_t e = cfd::adj::launch_rhs_vjp(h->fam, h->icst, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[0],
+                                             h->cfg.h[1], h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
+    h->launches += 2;
     return CFD_OK;
 }
 
@@ -1847,7 +1845,7 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
             if (!h->adj_rev_graph && (rc = capture_graph(h, [&] { return segment(K); }, &h->adj_rev_graph)))
                 return rc;
             CFD_CUDA(h, cudaGraphLaunch(h->adj_rev_graph, h->stream));
-            h->launches += (3ULL * h->dim + 18ULL) * K;
+            h->launches += (3ULL * h->dim + 12ULL) * K;
         } else if ((rc = segment(cnt))) {
             return rc;
         }
