@@ -29,15 +29,6 @@ namespace {
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// a read-only global load the compiler neither merges with an earlier load of
-// the same address nor moves
-__device__ __forceinline__ double ld_stream(const double *p)
-{
-    double x;
-    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(x) : "l"(p));
-    return x;
-}
-
 // one stencil position's contribution from the x face and the y face
 __device__ __forceinline__ double P_sum(const double *__restrict__ Px, const double *__restrict__ Py, long long off,
                                         long long fx, long long fy)
@@ -45,44 +36,109 @@ __device__ __forceinline__ double P_sum(const double *__restrict__ Px, const dou
     return Px[off + fx] + Py[off + fy];
 }
 
-// Face t of direction AX: P[(m * 4 + v) * ncell + t] = d(mu . R)/dU of stencil
-// cell m (face t lies before cell t along AX).
-template <int AX, int FAM>
-__device__ __forceinline__ void face_vjp_at(long long t, const double *__restrict__ u, const double *__restrict__ mu,
-                                            double *__restrict__ P, int nx, int ny, double inv_h, double ct)
-{
-    const long long ncell = (long long)nx * ny;
-    const int nd = (AX == 0) ? nx : ny;
-    const int x = (int)(t % nx), y = (int)(t / nx);
-    const int f = (AX == 0) ? x : y;
-    auto cell = [&](int pos) -> long long {
-        pos = wrap(pos, nd);
-        return (AX == 0) ? (long long)y * nx + pos : (long long)pos * nx + x;
-    };
-    // the stencil is read twice, once per half of the face adjoint: the
-    // volatile loads keep the compiler from holding the first copy in
-    // registers across the Roe flux's adjoint (where it would spill)
-    auto load_stencil = [&](double (&U)[6][4]) {
+// 128-thread CTAs per SM of the two face-adjoint halves. The first runs 4
+// (128 registers, ~0.3 KB of spills per thread: faster than 3 without
+// spills, and than 5); the second needs the full 255 (3 per SM, at 168
+// registers, spills 0.7-2.3 KB per thread and is 15% slower on the reverse)
+#ifndef ADJ_STATES_MINB
+#define ADJ_STATES_MINB 4
+#endif
+#ifndef ADJ_CHARS_MINB
+#define ADJ_CHARS_MINB 2
+#endif
+
+// The stencil of face t of direction AX (face t lies before cell t along AX)
+// and the face's adjoint weight Fb (the MND6 transpose applied to mu).
+template <int AX>
+struct FaceAt {
+    long long ncell, t, cells[6];
+    __device__ FaceAt(long long t_, int nx, int ny) : ncell((long long)nx * ny), t(t_)
+    {
+        const int nd = (AX == 0) ? nx : ny;
+        const int x = (int)(t % nx), y = (int)(t / nx);
+        const int f = (AX == 0) ? x : y;
 #pragma unroll
         for (int m = 0; m < 6; m++) {
-            const long long cm = cell(f - 3 + m);
-#pragma unroll
-            for (int v = 0; v < 4; v++) U[m][v] = ld_stream(u + v * ncell + cm);
+            const int pos = wrap(f - 3 + m, nd);
+            cells[m] = (AX == 0) ? (long long)y * nx + pos : (long long)pos * nx + x;
         }
-    };
-    FaceStates fs;
+    }
+    __device__ void stencil(const double *__restrict__ u, double (&U)[6][4]) const
     {
-        double U[6][4], Fb[4];
-        load_stencil(U);
-        const long long cm2 = cell(f - 2), cm1 = cell(f - 1), c0 = cell(f), cp1 = cell(f + 1);
+#pragma unroll
+        for (int m = 0; m < 6; m++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) U[m][v] = u[v * ncell + cells[m]];
+    }
+    __device__ void weight(const double *__restrict__ mu, double inv_h, double (&Fb)[4]) const
+    {
+        // cells f-2, f-1, f, f+1 are stencil positions 1..4
 #pragma unroll
         for (int v = 0; v < 4; v++)
-            Fb[v] = (kW0 * (mu[v * ncell + cm1] - mu[v * ncell + c0]) +
-                     kW2 * (mu[v * ncell + cm2] - mu[v * ncell + cp1])) * inv_h;
-        face_vjp_states<AX>(U, Fb, fs, FAM, ct);
+            Fb[v] = (kW0 * (mu[v * ncell + cells[2]] - mu[v * ncell + cells[3]]) +
+                     kW2 * (mu[v * ncell + cells[1]] - mu[v * ncell + cells[4]])) * inv_h;
+    }
+};
+
+// First half of the face adjoint (forward to the face states, Roe flux
+// adjoint): its FaceStates go to slots 0..23 of the face's P entries, the
+// eight 3-bit TENO flags to fl[t].
+template <int AX, int FAM>
+__device__ __forceinline__ void face_states_at(long long t, const double *__restrict__ u,
+                                               const double *__restrict__ mu, double *__restrict__ P,
+                                               unsigned *__restrict__ fl, int nx, int ny, double inv_h, double ct)
+{
+    const FaceAt<AX> fa(t, nx, ny);
+    double U[6][4], Fb[4];
+    fa.stencil(u, U);
+    fa.weight(mu, inv_h, Fb);
+    FaceStates fs;
+    face_vjp_states<AX>(U, Fb, fs, FAM, ct);
+    const long long n = fa.ncell;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        P[(0 + k) * n + t] = fs.QL[k];
+        P[(4 + k) * n + t] = fs.QR[k];
+        P[(8 + k) * n + t] = fs.clb[k];
+        P[(12 + k) * n + t] = fs.crb[k];
+        P[(16 + k) * n + t] = fs.P2b[k];
+        P[(20 + k) * n + t] = fs.P3b[k];
+    }
+    if (FAM != ADJ_WCNS5) {
+        unsigned w = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) w |= (fs.flL[k] << (3 * k)) | (fs.flR[k] << (12 + 3 * k));
+        fl[t] = w;
+    }
+}
+
+// Second half (characteristic projections, interpolations and eigensystem
+// backwards): reads the face's FaceStates from its P entries and overwrites
+// them with P[(m * 4 + v) * ncell + t] = d(mu . R)/dU of stencil cell m.
+template <int AX, int FAM>
+__device__ __forceinline__ void face_chars_at(long long t, const double *__restrict__ u, double *P,
+                                              const unsigned *__restrict__ fl, int nx, int ny)
+{
+    const FaceAt<AX> fa(t, nx, ny);
+    const long long n = fa.ncell;
+    FaceStates fs;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        fs.QL[k] = P[(0 + k) * n + t];
+        fs.QR[k] = P[(4 + k) * n + t];
+        fs.clb[k] = P[(8 + k) * n + t];
+        fs.crb[k] = P[(12 + k) * n + t];
+        fs.P2b[k] = P[(16 + k) * n + t];
+        fs.P3b[k] = P[(20 + k) * n + t];
+    }
+    const unsigned w = (FAM != ADJ_WCNS5) ? fl[t] : 0u;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        fs.flL[k] = (w >> (3 * k)) & 7u;
+        fs.flR[k] = (w >> (12 + 3 * k)) & 7u;
     }
     double U[6][4], Ub[6][4];
-    load_stencil(U);
+    fa.stencil(u, U);
 #pragma unroll
     for (int m = 0; m < 6; m++)
 #pragma unroll
@@ -91,21 +147,37 @@ __device__ __forceinline__ void face_vjp_at(long long t, const double *__restric
 #pragma unroll
     for (int m = 0; m < 6; m++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) P[(m * 4 + v) * ncell + t] = Ub[m][v];
+        for (int v = 0; v < 4; v++) P[(m * 4 + v) * n + t] = Ub[m][v];
 }
 
 // one thread per face, the faces of both directions in one launch (items
-// 0 .. ncell-1 along x into Px, ncell .. 2 ncell-1 along y into Py): twice the
-// work per launch keeps the register-heavy kernel's last wave short
+// 0 .. ncell-1 along x into Px, ncell .. 2 ncell-1 along y into Py); the two
+// halves of the face adjoint are two launches so that each fits in fewer
+// registers and runs more warps per SM
 template <int FAM>
-__global__ void face_vjp_kernel(const double *__restrict__ u, const double *__restrict__ mu, double *__restrict__ Px,
-                                double *__restrict__ Py, int nx, int ny, double inv_hx, double inv_hy, double ct)
+__global__ void __launch_bounds__(128, ADJ_STATES_MINB)
+    face_states_kernel(const double *__restrict__ u, const double *__restrict__ mu, double *__restrict__ Px,
+                       double *__restrict__ Py, unsigned *__restrict__ fl, int nx, int ny, double inv_hx,
+                       double inv_hy, double ct)
 {
     const long long ncell = (long long)nx * ny;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 2 * ncell;
          t += (long long)gridDim.x * blockDim.x) {
-        if (t < ncell) face_vjp_at<0, FAM>(t, u, mu, Px, nx, ny, inv_hx, ct);
-        else face_vjp_at<1, FAM>(t - ncell, u, mu, Py, nx, ny, inv_hy, ct);
+        if (t < ncell) face_states_at<0, FAM>(t, u, mu, Px, fl, nx, ny, inv_hx, ct);
+        else face_states_at<1, FAM>(t - ncell, u, mu, Py, fl + ncell, nx, ny, inv_hy, ct);
+    }
+}
+
+template <int FAM>
+__global__ void __launch_bounds__(128, ADJ_CHARS_MINB)
+    face_chars_kernel(const double *__restrict__ u, double *Px, double *Py, const unsigned *__restrict__ fl, int nx,
+                      int ny)
+{
+    const long long ncell = (long long)nx * ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 2 * ncell;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < ncell) face_chars_at<0, FAM>(t, u, Px, fl, nx, ny);
+        else face_chars_at<1, FAM>(t - ncell, u, Py, fl + ncell, nx, ny);
     }
 }
 
@@ -163,16 +235,25 @@ cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu
 {
     const long long ncell = (long long)nx * ny;
     double *Px = P, *Py = P + 24 * ncell;
+    unsigned *fl = reinterpret_cast<unsigned *>(P + 48 * ncell);
     const double ihx = 1.0 / hx, ihy = 1.0 / hy;
     const unsigned gf = grid_for(2 * ncell, 128);
-    if (fam == ADJ_WCNS5)
-        face_vjp_kernel<ADJ_WCNS5><<<gf, 128, 0, st>>>(u, mu, Px, Py, nx, ny, ihx, ihy, ct);
-    else if (fam == ADJ_TENOZ)
-        face_vjp_kernel<ADJ_TENOZ><<<gf, 128, 0, st>>>(u, mu, Px, Py, nx, ny, ihx, ihy, ct);
-    else if (fam == ADJ_TENOCONG)
-        face_vjp_kernel<ADJ_TENOCONG><<<gf, 128, 0, st>>>(u, mu, Px, Py, nx, ny, ihx, ihy, ct);
-    else
+    switch (fam) {
+    case ADJ_WCNS5:
+        face_states_kernel<ADJ_WCNS5><<<gf, 128, 0, st>>>(u, mu, Px, Py, fl, nx, ny, ihx, ihy, ct);
+        face_chars_kernel<ADJ_WCNS5><<<gf, 128, 0, st>>>(u, Px, Py, fl, nx, ny);
+        break;
+    case ADJ_TENOZ:
+        face_states_kernel<ADJ_TENOZ><<<gf, 128, 0, st>>>(u, mu, Px, Py, fl, nx, ny, ihx, ihy, ct);
+        face_chars_kernel<ADJ_TENOZ><<<gf, 128, 0, st>>>(u, Px, Py, fl, nx, ny);
+        break;
+    case ADJ_TENOCONG:
+        face_states_kernel<ADJ_TENOCONG><<<gf, 128, 0, st>>>(u, mu, Px, Py, fl, nx, ny, ihx, ihy, ct);
+        face_chars_kernel<ADJ_TENOCONG><<<gf, 128, 0, st>>>(u, Px, Py, fl, nx, ny);
+        break;
+    default:
         return cudaErrorInvalidValue;
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     gather_kernel<<<grid_for(ncell, 256), 256, 0, st>>>(u, mu, Px, Py, lam, nx, ny, ihx, ihy);

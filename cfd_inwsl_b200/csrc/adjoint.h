@@ -12,8 +12,9 @@ namespace adj {
 
 // lam = (dR/dU)^T mu, all arrays planar SoA [4][nx*ny]. fam: interpolation
 // family (0 WCNS5, 2 TENO-Z, 3 TENO-Cong) with constant ct; hx, hy the
-// spacings of the x and y differences. P is scratch of 48 * nx * ny doubles
-// (per-face contributions of both directions).
+// spacings of the x and y differences. P is scratch of 49 * nx * ny doubles
+// (per-face contributions of both directions, then one 32-bit word of TENO
+// flags per face).
 cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, double *lam, double *P, int nx,
                            int ny, double hx, double hy, cudaStream_t st);
 

@@ -17,6 +17,12 @@
 #define ADJ_HD inline
 #endif
 
+// unroll factor of the characteristic-field loop of the face adjoint's
+// second half
+#ifndef ADJ_CHARS_UNROLL
+#define ADJ_CHARS_UNROLL 4
+#endif
+
 namespace cfd {
 namespace adj {
 
@@ -27,6 +33,7 @@ constexpr double kGam = 1.4;  // GAMMA (macro.hpp)
 constexpr double kGm1 = kGam - 1.0;
 constexpr double kGG1 = kGam / (kGam - 1.0);
 constexpr double kW0 = 3.0 / 2.0, kW1 = -3.0 / 10.0, kW2 = 1.0 / 30.0;
+constexpr int kCharsUnroll = ADJ_CHARS_UNROLL;
 
 // cons (rho, rho u, rho v, rho E) -> prim (rho, u, v, p)
 ADJ_HD void c2p(const double *c, double *p)
@@ -437,7 +444,7 @@ ADJ_HD void face_vjp_chars(const double (&U)[6][4], const FaceStates &f, double 
     // eigenvector entries -> (u, v, h, c, ek, Vn, 1/c, 1/h); each row of L's
     // adjoint goes into these as soon as it is formed
     double ub = 0, vb = 0, hb = 0, cb = 0, ekb = 0, Vnb = 0, icb = 0, ihb = 0;
-#pragma unroll
+#pragma unroll kCharsUnroll
     for (int k = 0; k < 4; k++) {
         const double QLb = R[0][k] * clb[0] + R[1][k] * clb[1] + R[2][k] * clb[2] + R[3][k] * clb[3];
         const double QRb = R[0][k] * crb[0] + R[1][k] * crb[1] + R[2][k] * crb[2] + R[3][k] * crb[3];

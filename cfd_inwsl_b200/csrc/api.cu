@@ -1666,7 +1666,7 @@ int adjoint_buffers(cfd_handle *h)
     const size_t state = sizeof(double) * h->ncell * h->nv;
     for (int k = 0; k < 4; k++) {
         if (h->adj_buf[k]) continue;
-        cudaError_t e = cudaMalloc(&h->adj_buf[k], k == 3 ? 12 * state : state);
+        cudaError_t e = cudaMalloc(&h->adj_buf[k], k == 3 ? 12 * state + sizeof(double) * h->ncell : state);
         if (e != cudaSuccess) {
             h->adj_buf[k] = nullptr;
             return fail(h, CFD_ERR_NOMEM, "adjoint work buffers");
@@ -1682,7 +1682,7 @@ int rhs_vjp(cfd_handle *h, const double *U, const double *mu, double *w)
     cudaError_t e = cfd::adj::launch_rhs_vjp(h->fam, h->icst, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[0],
                                              h->cfg.h[1], h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
-    h->launches += 2;
+    h->launches += 3;
     return CFD_OK;
 }
 
@@ -1845,7 +1845,7 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
             if (!h->adj_rev_graph && (rc = capture_graph(h, [&] { return segment(K); }, &h->adj_rev_graph)))
                 return rc;
             CFD_CUDA(h, cudaGraphLaunch(h->adj_rev_graph, h->stream));
-            h->launches += (3ULL * h->dim + 12ULL) * K;
+            h->launches += (3ULL * h->dim + 15ULL) * K;
         } else if ((rc = segment(cnt))) {
             return rc;
         }
