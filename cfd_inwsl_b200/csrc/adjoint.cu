@@ -19,7 +19,8 @@
 // directions in one launch) recomputes the face forward in registers and runs
 // it backwards, writing its 6 x 4 contributions to a per-face buffer; a gather
 // kernel sums each cell's twelve face contributions and its two node
-// contributions (no atomics: the result is deterministic).
+// contributions (no atomics: the result is deterministic) and applies the
+// stage-adjoint combination the caller asks for.
 #include "adjoint.h"
 #include "adjoint_math.h"
 
@@ -182,9 +183,9 @@ __global__ void __launch_bounds__(128, ADJ_CHARS_MINB)
 }
 
 // one thread per cell: the six faces whose stencil holds it and its node flux,
-// in both directions; lam = the sum
+// in both directions; their sum g goes to o (VjpOut)
 __global__ void gather_kernel(const double *__restrict__ u, const double *__restrict__ mu,
-                              const double *__restrict__ Px, const double *__restrict__ Py, double *__restrict__ lam,
+                              const double *__restrict__ Px, const double *__restrict__ Py, const VjpOut o,
                               int nx, int ny, double inv_hx, double inv_hy)
 {
     const long long ncell = (long long)nx * ny;
@@ -211,14 +212,15 @@ __global__ void gather_kernel(const double *__restrict__ u, const double *__rest
         node_vjp<0>(U, Gx, acc);
         node_vjp<1>(U, Gy, acc);
 #pragma unroll
-        for (int v = 0; v < 4; v++) lam[v * ncell + t] = acc[v];
+        for (int v = 0; v < 4; v++) {
+            const long long i = v * ncell + t;
+            double r = o.b * acc[v];
+            if (o.x) r = o.a * o.x[i] + r;
+            if (o.z) r += o.e * o.z[i];
+            o.out[i] = r;
+            if (o.out2) o.out2[i] = o.c * o.out2[i] + o.d * o.y[i];
+        }
     }
-}
-
-__global__ void axpby_kernel(double a, const double *__restrict__ x, double b, double *__restrict__ y, long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        y[i] = a * x[i] + b * y[i];
 }
 
 unsigned grid_for(long long n, int threads)
@@ -230,8 +232,8 @@ unsigned grid_for(long long n, int threads)
 
 } // namespace
 
-cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, double *lam, double *P, int nx,
-                           int ny, double hx, double hy, cudaStream_t st)
+cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, const VjpOut &o, double *P,
+                           int nx, int ny, double hx, double hy, cudaStream_t st)
 {
     const long long ncell = (long long)nx * ny;
     double *Px = P, *Py = P + 24 * ncell;
@@ -256,13 +258,7 @@ cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    gather_kernel<<<grid_for(ncell, 256), 256, 0, st>>>(u, mu, Px, Py, lam, nx, ny, ihx, ihy);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_axpby(double a, const double *x, double b, double *y, long long n, cudaStream_t st)
-{
-    axpby_kernel<<<grid_for(n, 256), 256, 0, st>>>(a, x, b, y, n);
+    gather_kernel<<<grid_for(ncell, 256), 256, 0, st>>>(u, mu, Px, Py, o, nx, ny, ihx, ihy);
     return cudaGetLastError();
 }
 

@@ -10,16 +10,29 @@
 namespace cfd {
 namespace adj {
 
-// lam = (dR/dU)^T mu, all arrays planar SoA [4][nx*ny]. fam: interpolation
+// Where a product g = (dR/dU)^T mu goes, per entry i (the combinations of the
+// SSP-RK3 stage adjoints, applied as the product is formed):
+//   out[i] = a * x[i] + b * g[i] + e * z[i]     (x, z may be null: term absent)
+//   out2[i] = c * out2[i] + d * y[i]            (when out2 is not null)
+// out may be x or z. None of out, out2 may be mu: mu is read at neighbours.
+struct VjpOut {
+    double *out;
+    const double *x;
+    double a, b;
+    const double *z;
+    double e;
+    double *out2;
+    const double *y;
+    double c, d;
+};
+
+// (dR/dU)^T mu into o, all arrays planar SoA [4][nx*ny]. fam: interpolation
 // family (0 WCNS5, 2 TENO-Z, 3 TENO-Cong) with constant ct; hx, hy the
 // spacings of the x and y differences. P is scratch of 49 * nx * ny doubles
 // (per-face contributions of both directions, then one 32-bit word of TENO
 // flags per face).
-cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, double *lam, double *P, int nx,
-                           int ny, double hx, double hy, cudaStream_t st);
-
-// y = a * x + b * y over n doubles
-cudaError_t launch_axpby(double a, const double *x, double b, double *y, long long n, cudaStream_t st);
+cudaError_t launch_rhs_vjp(int fam, double ct, const double *u, const double *mu, const VjpOut &o, double *P,
+                           int nx, int ny, double hx, double hy, cudaStream_t st);
 
 } // namespace adj
 } // namespace cfd

@@ -1675,23 +1675,22 @@ int adjoint_buffers(cfd_handle *h)
     return CFD_OK;
 }
 
-// w = (dR/dU)^T mu at the state U (both directions)
-int rhs_vjp(cfd_handle *h, const double *U, const double *mu, double *w)
+// g = (dR/dU)^T mu at the state U (both directions) into o
+int rhs_vjp(cfd_handle *h, const double *U, const double *mu, const cfd::adj::VjpOut &o)
 {
     const int nx = h->cfg.n[0], ny = h->cfg.n[1];
-    cudaError_t e = cfd::adj::launch_rhs_vjp(h->fam, h->icst, U, mu, w, h->adj_buf[3], nx, ny, h->cfg.h[0],
+    cudaError_t e = cfd::adj::launch_rhs_vjp(h->fam, h->icst, U, mu, o, h->adj_buf[3], nx, ny, h->cfg.h[0],
                                              h->cfg.h[1], h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "adjoint sweep");
     h->launches += 3;
     return CFD_OK;
 }
 
-int axpby(cfd_handle *h, double a, const double *x, double b, double *y)
+// out = a x + b g + e z (x, z: nullptr when absent)
+cfd::adj::VjpOut vjp_out(double *out, const double *x = nullptr, double a = 0.0, double b = 1.0,
+                         const double *z = nullptr, double e = 0.0)
 {
-    cudaError_t e = cfd::adj::launch_axpby(a, x, b, y, h->ncell * h->nv, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint axpby");
-    h->launches += 1;
-    return CFD_OK;
+    return cfd::adj::VjpOut{out, x, a, b, z, e, nullptr, nullptr, 0.0, 0.0};
 }
 
 void adjoint_release(std::vector<double *> &v)
@@ -1730,7 +1729,7 @@ int cfd_rhs_vjp(cfd_handle *h, const double *mu_aos, double *lam_aos)
     CFD_CUDA(h, cudaMemcpyAsync(h->stage, mu_aos, sizeof(double) * h->ncell * h->nv, cudaMemcpyHostToDevice,
                                 h->stream));
     if ((rc = launch_aos_to_soa(h, h->stage, h->adj_buf[0]))) return rc;
-    if ((rc = rhs_vjp(h, h->u[h->cur], h->adj_buf[0], h->adj_buf[1]))) return rc;
+    if ((rc = rhs_vjp(h, h->u[h->cur], h->adj_buf[0], vjp_out(h->adj_buf[1])))) return rc;
     if ((rc = launch_soa_to_aos(h, h->adj_buf[1], h->stage, 0))) return rc;
     CFD_CUDA(h, cudaMemcpyAsync(lam_aos, h->stage, sizeof(double) * h->ncell * h->nv, cudaMemcpyDeviceToHost,
                                 h->stream));
@@ -1821,15 +1820,14 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
         //   U1 = U0 - dt R(U0); U2 = 3/4 U0 + 1/4 (U1 - dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 - dt R(U2))
         for (int j = cnt - 1; j >= 0; j--) {
             double *U0 = h->adj_stage[3 * j], *U1 = h->adj_stage[3 * j + 1], *U2 = h->adj_stage[3 * j + 2];
-            if ((r = rhs_vjp(h, U2, lam, w))) return r;                 // w = J(U2)^T lam3
-            if ((r = axpby(h, 2.0 / 3.0, lam, -2.0 / 3.0 * dt, w))) return r;  // w = lam2
-            if ((r = axpby(h, 0.0, lam, 1.0 / 3.0, lam))) return r;     // lam = lam3 / 3
-            if ((r = rhs_vjp(h, U1, w, w2))) return r;                  // w2 = J(U1)^T lam2
-            if ((r = axpby(h, 0.25, w, -0.25 * dt, w2))) return r;      // w2 = lam1
-            if ((r = axpby(h, 0.75, w, 1.0, lam))) return r;            // lam += 3/4 lam2
-            if ((r = rhs_vjp(h, U0, w2, w))) return r;                  // w = J(U0)^T lam1
-            if ((r = axpby(h, 1.0, w2, 1.0, lam))) return r;            // lam += lam1
-            if ((r = axpby(h, -dt, w, 1.0, lam))) return r;             // lam -= dt w
+            // lam2 = 2/3 (lam3 - dt J(U2)^T lam3)
+            if ((r = rhs_vjp(h, U2, lam, vjp_out(w, lam, 2.0 / 3.0, -2.0 / 3.0 * dt)))) return r;
+            // lam1 = 1/4 (lam2 - dt J(U1)^T lam2); lam = lam3 / 3 + 3/4 lam2
+            cfd::adj::VjpOut o1 = vjp_out(w2, w, 0.25, -0.25 * dt);
+            o1.out2 = lam; o1.c = 1.0 / 3.0; o1.y = w; o1.d = 0.75;
+            if ((r = rhs_vjp(h, U1, w, o1))) return r;
+            // lam0 = lam + lam1 - dt J(U0)^T lam1
+            if ((r = rhs_vjp(h, U0, w2, vjp_out(lam, lam, 1.0, -dt, w2, 1.0)))) return r;
         }
         return CFD_OK;
     };
@@ -1845,7 +1843,7 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
             if (!h->adj_rev_graph && (rc = capture_graph(h, [&] { return segment(K); }, &h->adj_rev_graph)))
                 return rc;
             CFD_CUDA(h, cudaGraphLaunch(h->adj_rev_graph, h->stream));
-            h->launches += (3ULL * h->dim + 15ULL) * K;
+            h->launches += (3ULL * h->dim + 9ULL) * K;
         } else if ((rc = segment(cnt))) {
             return rc;
         }
