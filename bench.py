@@ -218,7 +218,7 @@ def vortex_accuracy(n, L, im, fm, cfl, device, t_end=2.0):
 def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
     """Adjoint configuration: 256^2 periodic [0,1]^2, rho = 1 + drho (seeded
     Gaussian-filtered noise, correlation length 0.05, RMS 1e-2), p = 1/gamma,
-    (u, v) = (0.5, 0.3), WCNS5 + Roe, 400 frozen-dt RK3 steps (dt from CFL 0.5 at
+    (u, v) = (0.5, 0.3), WCNS5 + Roe, nsteps (400) frozen-dt RK3 steps (dt from CFL 0.5 at
     t = 0), checkpoints every 20 steps, J = sum of rho^2 over 64 seeded probe
     cells. Times, with CUDA events on the handle's stream: the forward steps,
     cfd_adjoint_record (forward with checkpoints) and cfd_adjoint_reverse
@@ -269,14 +269,14 @@ def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
     rev_ms = timed(lambda: out.setdefault("g", s.adjoint_reverse(seed_g)))
     J = float(np.sum(UN[probes, 0] ** 2))
     s.close()
-    return {"config": "256^2 periodic, WCNS5 + Roe, 400 frozen-dt RK3 steps, checkpoints every 20, "
+    return {"config": f"{n}^2 periodic, WCNS5 + Roe, {nsteps} frozen-dt RK3 steps, checkpoints every {ckpt}, "
                       "J = sum of rho^2 over 64 probes",
             "forward_ms": fwd_ms, "record_ms": rec_ms, "reverse_ms": rev_ms,
             "reverse_over_forward": rev_ms / fwd_ms, "record_plus_reverse_over_forward": (rec_ms + rev_ms) / fwd_ms,
             # the record pass is itself a forward run (graph-replayed, plus the
             # checkpoint copies): the reverse pass against the fastest forward
             "reverse_over_record": rev_ms / rec_ms,
-            "forward": "400 cfd_rk3_step calls (the per-step API, one host sync each)",
+            "forward": f"{nsteps} cfd_rk3_step calls (the per-step API, one host sync each)",
             "J": J, "grad_l2": float(np.linalg.norm(out["g"]))}
 
 
@@ -565,7 +565,7 @@ def run_ours(args, rank, world, local_rank):
 
     adjoint = None
     if not args.no_adjoint and world == 1:
-        adjoint = adjoint_cost(local_rank, stream)
+        adjoint = adjoint_cost(local_rank, stream, nsteps=args.adjoint_steps)
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_throughput(local_rank, stream)
@@ -636,9 +636,18 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="form of the timed steps (mixed: CFD_PREC_MIXED)")
     ap.add_argument("--accuracy-grid", type=int, default=512)
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint cost measurement and print its dict (for profiling the adjoint kernels)")
+    ap.add_argument("--adjoint-steps", type=int, default=400, help="RK3 steps of the adjoint measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(0)
+        r = adjoint_cost(0, torch.cuda.Stream(), nsteps=args.adjoint_steps)
+        print(json.dumps({"adjoint": r}), flush=True)
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
