@@ -20,8 +20,12 @@ analytic field.
           bounded sample of the same workload, on this host's cores.
 
 --impl reference runs only the reference CPU solver on the same workload.
-For --gpus N > 1 every rank advances its own grid (independent replicas, no
-data-path collective); value = all ranks' cell-steps / max rank time.
+For --gpus N > 1 (one process per GPU under torchrun) the ranks share one
+periodic grid split into slabs along the last direction, each rank an n^dim
+tile (weak scaling): before every RK stage neighbouring slabs exchange their
+four boundary rows by NCCL point-to-point, and every step takes dt from a MAX
+all-reduce of the ranks' wave speeds; value = all ranks' cell-steps / max rank
+time.
 """
 from __future__ import annotations
 

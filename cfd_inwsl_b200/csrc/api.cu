@@ -25,6 +25,11 @@
 using cfd::BcLine;
 using cfd::SweepParams;
 
+namespace cfd {
+int default_seg_len_for(const cfd_config *cfg, int fam, bool strict, int d);
+bool config_bc_ok(const cfd_config *cfg, const char **why);
+}
+
 namespace {
 
 constexpr int kGhost = 4;
@@ -533,32 +538,7 @@ int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, doub
 
 int default_seg_len(const cfd_handle *h, int d)
 {
-    int n = h->cfg.n[d];
-    int S = (h->dim == 1) ? cfd::k1S : (d == 0 ? cfd::kXS : cfd::kYS);
-    int W = (h->dim == 1) ? cfd::k1W : (d == 0 ? cfd::kXW : cfd::kYW);
-    if (h->dim > 1 && d == 0 && h->cfg.diff_method != CFD_DIFF_TRAD6 &&
-        (h->dim == 3 || h->cfg.precision == CFD_PREC_FP64)) {
-        S = cfd::kXSn;  // the x sweep shape of launch_sweep
-        W = cfd::kXWn;
-    }
-    const bool mixed_shape = (d == 1 || (d == 2 && CFD_MIXED_Z16)) && h->cfg.precision == CFD_PREC_MIXED && !h->strict &&
-                             h->fam != cfd::FAM_RESEARCH;
-    const bool fp64_shape = h->cfg.precision == CFD_PREC_FP64 &&
-                            ((CFD_FP64_3D_YZ16 && h->dim == 3 && d > 0) || (CFD_FP64_2D_Y16 && h->dim == 2 && d == 1));
-    if (h->dim > 1 && (mixed_shape || fp64_shape) && h->cfg.diff_method != CFD_DIFF_TRAD6) {
-        S = cfd::kYSm;  // the mixed form's y sweep shape (launch_sweep)
-        W = cfd::kYWm;
-    }
-    int t0, t1;
-    transverse_axes(d, t0, t1);
-    long long blocks_per_seg = (long long)((h->cfg.n[t0] + W - 1) / W) * h->cfg.n[t1];
-    // about 1,800 CTAs (3 to 6 waves at 2 to 4 resident per SM); the mixed
-    // form's x sweep measured fastest with half as many, longer segments
-    const bool mixed_x = d == 0 && h->dim > 1 && h->cfg.precision == CFD_PREC_MIXED;
-    const long long target = mixed_x ? 148LL * 2 * 3 : 148LL * 2 * 6;
-    int seg = n;
-    while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
-    return seg;
+    return cfd::default_seg_len_for(&h->cfg, h->fam, h->strict, d);
 }
 
 
@@ -723,6 +703,11 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     }
     InterMap im = map_inter_method(cfg->inter_method, cfg->dim);
     if (!im.ok) return CFD_ERR_UNSUPPORTED;
+    const char *why = nullptr;
+    if (!cfd::config_bc_ok(cfg, &why)) {
+        fprintf(stderr, "cfd_create: %s\n", why);
+        return CFD_ERR_CONFIG;
+    }
 
     cfd_handle *h = new cfd_handle();
     h->cfg = *cfg;
@@ -819,6 +804,10 @@ int cfd_set_line_bc(cfd_handle *h, int idim, int i, int j, int side, int bnd_typ
     transverse_axes(d, t0, t1);
     if (i < 0 || i >= h->cfg.n[t0] || j < 0 || j >= h->cfg.n[t1]) return fail(h, CFD_ERR_CONFIG, "line index out of range");
     if (bnd_type == CFD_BND_HALO) return fail(h, CFD_ERR_CONFIG, "halo ends are wired by cfd_enable_halo");
+    // BndType values (macro.hpp:33-34) and the true wrap; anything else would
+    // leave the line end's ghosts undefined
+    if (!((bnd_type >= CFD_BND_TYPENULL && bnd_type <= CFD_BND_SYMMETRYZ) || bnd_type == CFD_BND_PERIODIC_WRAP))
+        return fail(h, CFD_ERR_CONFIG, "unknown boundary type");
     if (bnd_type != CFD_BND_PERIODIC_WRAP && (i0 < 0 || i0 >= h->ncell)) return fail(h, CFD_ERR_CONFIG, "i0 out of range");
     if (bnd_type == CFD_BND_PERIODIC1D || (bnd_type >= CFD_BND_SYMMETRYX && bnd_type <= CFD_BND_SYMMETRYZ) ||
         bnd_type == CFD_BND_SYMMETRY1D) {
@@ -1159,8 +1148,80 @@ extern "C" int cfd_accuracy_test(int inter_method, int n, double h, const double
     return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
 }
 
-// Selector lookup shared with the allocation-free entry point (noalloc.cu).
 namespace cfd {
+// Default cells per CTA segment along direction d for the tile shapes that
+// launch_sweep picks for this configuration: about six waves of CTAs over the
+// 148 SMs. Shared with the allocation-free entry point (noalloc.cu).
+int default_seg_len_for(const cfd_config *cfg, int fam, bool strict, int d)
+{
+    int n = cfg->n[d];
+    int S = (cfg->dim == 1) ? cfd::k1S : (d == 0 ? cfd::kXS : cfd::kYS);
+    int W = (cfg->dim == 1) ? cfd::k1W : (d == 0 ? cfd::kXW : cfd::kYW);
+    if (cfg->dim > 1 && d == 0 && cfg->diff_method != CFD_DIFF_TRAD6 &&
+        (cfg->dim == 3 || cfg->precision == CFD_PREC_FP64)) {
+        S = cfd::kXSn;  // the x sweep shape of launch_sweep
+        W = cfd::kXWn;
+    }
+    const bool mixed_shape = (d == 1 || (d == 2 && CFD_MIXED_Z16)) && cfg->precision == CFD_PREC_MIXED && !strict &&
+                             fam != cfd::FAM_RESEARCH;
+    const bool fp64_shape = cfg->precision == CFD_PREC_FP64 &&
+                            ((CFD_FP64_3D_YZ16 && cfg->dim == 3 && d > 0) || (CFD_FP64_2D_Y16 && cfg->dim == 2 && d == 1));
+    if (cfg->dim > 1 && (mixed_shape || fp64_shape) && cfg->diff_method != CFD_DIFF_TRAD6) {
+        S = cfd::kYSm;  // the mixed form's y sweep shape (launch_sweep)
+        W = cfd::kYWm;
+    }
+    int t0, t1;
+    transverse_axes(d, t0, t1);
+    long long blocks_per_seg = (long long)((cfg->n[t0] + W - 1) / W) * cfg->n[t1];
+    // about 1,800 CTAs (3 to 6 waves at 2 to 4 resident per SM); the mixed
+    // form's x sweep measured fastest with half as many, longer segments
+    const bool mixed_x = d == 0 && cfg->dim > 1 && cfg->precision == CFD_PREC_MIXED;
+    const long long target = mixed_x ? 148LL * 2 * 3 : 148LL * 2 * 6;
+    int seg = n;
+    while (blocks_per_seg * ((n + seg - 1) / seg) < target && seg > 4 * S) seg = (seg + 1) / 2;
+    return seg;
+}
+
+// The boundary types cfg->bc can wire by itself, i.e. every line end of a
+// direction with no per-line data: the copying types (PERIODIC1D and
+// SUPERSONICOUTLET with the Initializer::initBnds source cells, the true
+// wrap), the mirrors of the directions the grid has (SYMMETRY1D in 1D only:
+// in 2D and 3D it leaves the pressure ghost to static data), and the moving
+// DoubleMachUp top in 2D. DIRICLET and the other static types need ghost
+// values (cfd_set_line_bc), HALO ends are wired by cfd_enable_halo, and any
+// other value is not a BndType (macro.hpp:33-34). Checked before any device
+// work: a line end of one of those types would read ghost data that does not
+// exist (all-zero ghosts, or a null halo buffer).
+bool config_bc_ok(const cfd_config *cfg, const char **why)
+{
+    for (int d = 0; d < cfg->dim; d++)
+        for (int s = 0; s < 2; s++) {
+            const int t = cfg->bc[d][s];
+            bool ok = false;
+            switch (t) {
+            case CFD_BND_PERIODIC1D:
+            case CFD_BND_SUPERSONICOUTLET:
+            case CFD_BND_PERIODIC_WRAP:
+            case CFD_BND_SYMMETRYX: ok = true; break;
+            case CFD_BND_SYMMETRY1D: ok = cfg->dim == 1; break;
+            case CFD_BND_SYMMETRYY: ok = cfg->dim >= 2; break;
+            case CFD_BND_SYMMETRYZ: ok = cfg->dim == 3; break;
+            case CFD_BND_DOUBLEMACHUP: ok = cfg->dim == 2; break;
+            default: ok = false;
+            }
+            if (!ok) {
+                if (why)
+                    *why = (t == CFD_BND_HALO) ? "CFD_BND_HALO in cfg->bc (halo ends are wired by cfd_enable_halo)"
+                           : (t == CFD_BND_DIRICLET || t == CFD_BND_TYPENULL || (t >= 4 && t <= 6) || t == 9)
+                               ? "a static boundary type in cfg->bc (its ghost values are set per line by cfd_set_line_bc)"
+                               : "cfg->bc holds a boundary type this dimension cannot wire";
+                return false;
+            }
+        }
+    return true;
+}
+
+// Selector lookup shared with the allocation-free entry point (noalloc.cu).
 bool map_inter_method_for(int inter_method, int dim, int *fam, double *c)
 {
     InterMap im = map_inter_method(inter_method, dim);

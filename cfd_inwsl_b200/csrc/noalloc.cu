@@ -19,6 +19,8 @@
 
 namespace cfd {
 bool map_inter_method_for(int inter_method, int dim, int *fam, double *c);
+int default_seg_len_for(const cfd_config *cfg, int fam, bool strict, int d);
+bool config_bc_ok(const cfd_config *cfg, const char **why);
 }
 
 namespace {
@@ -111,6 +113,21 @@ extern "C" int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, do
     int fam;
     double icst;
     if (!cfd::map_inter_method_for(cfg->inter_method, cfg->dim, &fam, &icst)) return CFD_ERR_UNSUPPORTED;
+    const char *why = nullptr;
+    if (!cfd::config_bc_ok(cfg, &why)) {
+        fprintf(stderr, "cfd_rhs_noalloc: %s\n", why);
+        return CFD_ERR_CONFIG;
+    }
+    // An error left pending by earlier, unrelated work on this thread is not
+    // ours to report or to clear: refuse to queue anything behind it.
+    {
+        cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess) {
+            fprintf(stderr, "cfd_rhs_noalloc: an earlier CUDA error is pending (%s); nothing was queued\n",
+                    cudaGetErrorString(pending));
+            return CFD_ERR_CUDA;
+        }
+    }
 
     const long long ncell = (long long)cfg->n[0] * cfg->n[1] * cfg->n[2];
     WireArgs w;
@@ -185,7 +202,7 @@ extern "C" int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, do
         p.t = t;
         p.icst = icst;
         p.icst_k = (fam == cfd::FAM_TENOZ) ? cfd::teno_kappa(icst) : 0.0;
-        p.seg_len = cfg->seg_len[d] > 0 ? cfg->seg_len[d] : cfg->n[d];
+        p.seg_len = cfg->seg_len[d] > 0 ? cfg->seg_len[d] : cfd::default_seg_len_for(cfg, fam, cfg->strict != 0, d);
         p.dm_u = 8.25 * std::cos(M_PI / 6);
         p.dm_v = -8.25 * std::sin(M_PI / 6);
         p.gravity = (cfg->source_type == 1 && d == cfg->dim - 1) ? 1 : 0;

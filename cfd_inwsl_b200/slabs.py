@@ -125,6 +125,34 @@ class Slab:
         _lib.check(self.lib.cfd_rk3_stage(self.solver.h, stage, float(dt), float(t)), self.solver.h)
 
 
+def words_from_wave_speeds(lam) -> np.ndarray:
+    """Non-negative doubles as the int64 reduction words the library keeps
+    (their IEEE bit patterns, which order like the integers)."""
+    a = np.ascontiguousarray(np.asarray(lam, dtype=np.float64))
+    if np.any(np.signbit(a)) or np.any(np.isnan(a)):
+        raise ValueError("reduction words hold non-negative, non-NaN doubles")
+    return a.view(np.int64).copy()
+
+
+def wave_speeds_from_words(words) -> np.ndarray:
+    """Inverse of words_from_wave_speeds."""
+    return np.ascontiguousarray(np.asarray(words, dtype=np.int64)).view(np.float64).copy()
+
+
+def allreduce_max_words(dist, group, words):
+    """Global maxima of every rank's reduction words ([0] max |R_rho|, [1..3]
+    max (c + |u_d|) / h_d), in place: a MAX all-reduce of the int64 bit
+    patterns is the maximum of the doubles they encode."""
+    dist.all_reduce(words, op=dist.ReduceOp.MAX, group=group)
+    return words
+
+
+def dt_from_words(words, dim: int, cfl: float) -> float:
+    """The step the device's step control takes from the (reduced) words:
+    CFL / sum_d lambda_d (getTimeIntervalExplicit, blockSolver.cpp:318-349)."""
+    return dt_from_wave_speeds(wave_speeds_from_words(words)[1:1 + dim], dim, cfl)
+
+
 def dt_from_wave_speeds(lam, dim: int, cfl: float) -> float:
     """getTimeIntervalExplicit's CFL / sum_d max (c + |u_d|) / h_d, summed in direction order."""
     total = 0.0
@@ -252,7 +280,7 @@ class SlabRank:
             _lib.check(lib.cfd_loop_begin(h, float(cfl), float(t)), h)
             words = self.slab.reduction_words()
             for _ in range(steps):
-                self.dist.all_reduce(words, op=self.dist.ReduceOp.MAX, group=self.group)
+                allreduce_max_words(self.dist, self.group, words)
                 _lib.check(lib.cfd_loop_step_begin(h), h)
                 for stage in (1, 2, 3):
                     exchange_rows(self.dist, self.group, self.rank, self.nb, self.slab.stage_state(stage),

@@ -163,6 +163,12 @@ class Info:
         return {DiffMethod.MND6: 4, DiffMethod.TRAD6: 5, DiffMethod.HDS6: 3}.get(DiffMethod(self.diffMethod), 0)
 
 
+# BndTypes whose OneDBnd::update is a no-op (the ghosts keep static data set by
+# OneDBnd::setValue): cfd_config.bc cannot wire them by itself.
+STATIC_BND_TYPES = frozenset({BndType.TYPENULL, BndType.DIRICLET, BndType.DIRICLET_SODL, BndType.DIRICLET_SODR,
+                              BndType.FLUXGHOST, BndType.ARDBND})
+
+
 def default_bc_types(info: Info) -> list[list[int]]:
     """Per direction/side BndType of Initializer::initBnds for Euler
     (initializer.cpp:775-811): outlets by default, mirrors for nCase 2,
@@ -207,9 +213,18 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
     types = bc if bc is not None else default_bc_types(info)
     if periodic:
         types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]
+    # sides of a named case whose lines wire_case_bnds sets one by one
+    per_line = bc is None and not periodic and info.dim == 2 and info.nCase in (3, 4)
     for d in range(3):
         for s in range(2):
-            cfg.bc[d][s] = int(types[d][s])
+            t = int(types[d][s])
+            if d < info.dim and t in STATIC_BND_TYPES:
+                if not per_line:
+                    raise ValueError(f"boundary type {BndType(t).name} (direction {d}, side {s}) needs ghost "
+                                     "values per line: wire it with set_line_bc")
+                # provisional wiring of cfd_create; wire_case_bnds replaces every line of this side
+                t = int(BndType.SUPERSONICOUTLET)
+            cfg.bc[d][s] = t
     return cfg
 
 

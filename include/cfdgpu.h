@@ -90,7 +90,12 @@ typedef struct cfd_config {
     int bc[3][2];       /* default boundary type per direction and side (0 = low, 1 = high),
                            wired per line like Initializer::initBnds (initializer.cpp:743-870):
                            low side i0 = first cell, offset = +stride (calOffset);
-                           high side i0 = last cell, offset = -stride (calOffsetInverse) */
+                           high side i0 = last cell, offset = -stride (calOffsetInverse).
+                           Accepted here (CFD_ERR_CONFIG otherwise, before any device work):
+                           PERIODIC1D, SUPERSONICOUTLET, PERIODIC_WRAP, SYMMETRYX, SYMMETRY1D (1D),
+                           SYMMETRYY (2D/3D), SYMMETRYZ (3D), DOUBLEMACHUP (2D). Static types such
+                           as DIRICLET need ghost values: wire those lines with cfd_set_line_bc.
+                           HALO ends are wired by cfd_enable_halo. */
     int device;         /* CUDA device ordinal */
     int seg_len[3];     /* cells per CTA segment along each sweep (0 = autotuned default) */
     int source_type;    /* SourceType (macro.hpp:90): 0 none, 1 GRAVITY (2D; SourceTerm::calGravitySource,
@@ -201,7 +206,12 @@ int cfd_eval_face(int dim, int ax, int inter_method, int precision, const double
  * 4096 x 4096 fit) are rejected with CFD_ERR_CONFIG and a message on stderr.
  * The first call on a device looks up the array's device address (once per
  * device, with cfg->device made current); make that first call before any
- * stream capture. Every call rewrites the part of the array it uses, and all
+ * stream capture. The address is kept until the process exits: after
+ * cudaDeviceReset, or anything else that destroys the device's primary
+ * context, this entry point must not be called on that device again in the
+ * same process. cfg->bc takes the same types as in cfd_create. A CUDA error
+ * already pending on the calling thread is left in place and the call
+ * returns CFD_ERR_CUDA without queueing anything. Every call rewrites the part of the array it uses, and all
  * calls share it: calls that overlap on the GPU (different streams, or other
  * threads) race on the array and must be serialised by the caller. */
 #define CFD_NOALLOC_MAX_LINE_ENDS 16384

@@ -27,6 +27,7 @@ file the reference repository commits:
 from __future__ import annotations
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -39,7 +40,7 @@ sys.path.insert(0, str(ROOT))
 
 from oracle.refsolver import RefSolver, ref_flux, ref_inter5, ref_recon_face  # noqa: E402
 
-REF_ROOT = Path("/root/reference")
+REF_ROOT = Path(os.environ.get("CFD_REFERENCE_ROOT", "/root/reference"))
 INTER_METHODS = [2, 3, 8, 9, 10, 11, 12, 13, 15, 22, 23, 35, 37]
 GAMMA = 1.4
 

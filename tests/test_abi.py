@@ -74,3 +74,64 @@ def test_small_grid_rejected():
 
 def test_version_string():
     assert b"sm_100a" in _lib.load().cfd_version()
+
+
+@pytest.mark.parametrize("dim,d,value", [
+    (2, 1, 101),  # CFD_BND_HALO: wired by cfd_enable_halo only
+    (2, 0, 3),    # DIRICLET: needs ghost values per line
+    (2, 1, 0),    # TYPENULL: static data as well
+    (2, 0, 57),   # not a BndType
+    (2, 0, 2),    # SYMMETRY1D outside 1D leaves the pressure ghost undefined
+    (2, 1, 12),   # SYMMETRYZ in 2D
+    (3, 2, 8),    # DoubleMachUp is a 2D boundary
+    (1, 0, 11),   # SYMMETRYY in 1D
+])
+def test_config_boundary_types_rejected_without_gpu(dim, d, value):
+    """cfg->bc may only hold types the configuration can wire by itself; the
+    rest is refused with CFD_ERR_CONFIG before any device call, by cfd_create
+    and by the allocation-free entry point (dummy pointers: nothing is read)."""
+    lib, cfg = _cfg(dim=dim)
+    for k in range(3):
+        cfg.n[k] = 16 if k < dim else 1
+    cfg.bc[d][1] = value
+    h = C.c_void_p()
+    assert lib.cfd_create(C.byref(cfg), C.byref(h)) == -1
+    assert not h.value
+    dummy = C.c_void_p(0x1000)
+    assert lib.cfd_rhs_noalloc(C.byref(cfg), dummy, dummy, C.c_double(0.0), None) == -1
+
+
+def test_valid_boundary_types_pass_validation_without_gpu():
+    """Accepted types get past validation and fail only at the first CUDA call
+    here (no device): CFD_ERR_CUDA, not CFD_ERR_CONFIG."""
+    if _lib_has_gpu():
+        pytest.skip("a device is present")
+    for dim, types in ((1, [2, 7]), (2, [1, 7, 10, 11, 8, 100]), (3, [12, 10, 11, 100])):
+        lib, cfg = _cfg(dim=dim)
+        for k in range(3):
+            cfg.n[k] = 16 if k < dim else 1
+        for t in types:
+            for d in range(dim):
+                if t == 8 and d != 1:
+                    continue
+                cfg.bc[d][0] = t
+                h = C.c_void_p()
+                assert lib.cfd_create(C.byref(cfg), C.byref(h)) == -2, (dim, d, t)
+                cfg.bc[d][0] = 7
+
+
+def _lib_has_gpu():
+    from tests.conftest import gpu_available
+    return gpu_available()
+
+
+def test_make_config_refuses_static_types_without_per_line_wiring():
+    from cfd_inwsl_b200 import zone
+    info = zone.Info()
+    info.dim = 2
+    info.iMax = [17, 17, 1]
+    with pytest.raises(ValueError):
+        zone.make_config(info, bc=[[zone.BndType.DIRICLET] * 2, [7, 7], [7, 7]])
+    info.nCase = 3  # RTI: the Dirichlet rows are wired line by line after cfd_create
+    cfg = zone.make_config(info)
+    assert list(cfg.bc[1]) == [int(zone.BndType.SUPERSONICOUTLET)] * 2

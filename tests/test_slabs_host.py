@@ -75,3 +75,83 @@ def test_exchange_rows_gloo(world, periodic):
             assert got[1] is None
         else:  # the high neighbour's first GHOST rows
             np.testing.assert_array_equal(got[1], state_of(hi).numpy()[:, :GHOST, :])
+
+
+# ------------------------------------------------------------- dt over the ranks
+GAMMA = 1.4
+
+
+def local_words(rank, nrows, rowlen, dim, h):
+    """Reduction words of one rank's slab of a random state: [0] a stand-in for
+    max |R_rho|, [1..dim] max_cells (c + |u_d|) / h_d as the sweep epilogue
+    reduces them (getTimeIntervalExplicit, blockSolver.cpp:318-349)."""
+    rng = np.random.default_rng(100 + rank)
+    ncell = nrows * rowlen
+    rho = rng.uniform(0.1, 2.0, ncell)
+    vel = rng.uniform(-1.0, 1.0, (dim, ncell)) * (10.0 ** rng.integers(-3, 2))
+    p = rng.uniform(0.05, 2.0, ncell)
+    c = np.sqrt(GAMMA * p / rho)
+    lam = [np.max((c + np.abs(vel[d])) / h[d]) for d in range(dim)]
+    words = [rng.uniform(0, 1) * 10.0 ** rng.integers(-300, 300)] + lam + [0.0] * (3 - dim)
+    return np.array(words), (rho, vel, p)
+
+
+def _dt_worker(rank, world, port, dim, out):
+    from cfd_inwsl_b200.slabs import allreduce_max_words, dt_from_words, words_from_wave_speeds
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        h = [0.01, 0.02, 0.005][:dim]
+        vals, _ = local_words(rank, 6, 9, dim, h)
+        words = torch.from_numpy(words_from_wave_speeds(vals))
+        allreduce_max_words(dist, None, words)
+        out[rank] = (words.numpy().copy(), dt_from_words(words.numpy(), dim, 0.5))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dim", [(2, 2), (3, 3), (3, 2)])
+def test_dt_from_max_allreduce_of_words_gloo(world, dim):
+    """The per-step MAX all-reduce of the int64 reduction words gives every
+    rank the global maxima bit for bit, and the dt built from them equals the
+    reference formula CFL / sum_d max (c + |u_d|) / h_d over the undivided grid."""
+    from cfd_inwsl_b200.slabs import wave_speeds_from_words
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_dt_worker, args=(world, port, dim, out), nprocs=world, start_method="spawn")
+    h = [0.01, 0.02, 0.005][:dim]
+    per_rank = [local_words(r, 6, 9, dim, h) for r in range(world)]
+    want = np.max([w for w, _ in per_rank], axis=0)
+    # the undivided grid: every rank's cells together
+    rho = np.concatenate([s[0] for _, s in per_rank])
+    vel = np.concatenate([s[1] for _, s in per_rank], axis=1)
+    p = np.concatenate([s[2] for _, s in per_rank])
+    c = np.sqrt(GAMMA * p / rho)
+    lam_total = 0.0
+    for d in range(dim):
+        lam_total += np.max((c + np.abs(vel[d])) / h[d])
+    dt_whole = 0.5 / lam_total
+    for r in range(world):
+        words, dt = out[r]
+        np.testing.assert_array_equal(wave_speeds_from_words(words), want)
+        assert dt == dt_whole
+
+
+def test_words_order_like_the_doubles():
+    """IEEE bit patterns of non-negative doubles order like the doubles,
+    subnormals, zero and huge values included; negative or NaN inputs are refused."""
+    from cfd_inwsl_b200.slabs import wave_speeds_from_words, words_from_wave_speeds
+    vals = np.array([0.0, 5e-324, 2.2e-308, 1e-300, 0.5, 1.0, 1.0000000000000002, 3e10, 1e308, np.inf])
+    w = words_from_wave_speeds(vals)
+    assert np.all(np.diff(w) > 0)
+    np.testing.assert_array_equal(wave_speeds_from_words(w), vals)
+    rng = np.random.default_rng(5)
+    a, b = rng.uniform(0, 1e6, 1000), rng.uniform(0, 1e6, 1000)
+    np.testing.assert_array_equal(wave_speeds_from_words(np.maximum(words_from_wave_speeds(a),
+                                                                    words_from_wave_speeds(b))), np.maximum(a, b))
+    with pytest.raises(ValueError):
+        words_from_wave_speeds([-1.0])
+    with pytest.raises(ValueError):
+        words_from_wave_speeds([np.nan])

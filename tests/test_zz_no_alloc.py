@@ -77,3 +77,38 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     cfg.h[0] = cfg.h[1] = 1.0 / 8192
     dummy = C.c_void_p(1)
     assert lib.cfd_rhs_noalloc(C.byref(cfg), dummy, dummy, 0.0, None) == -1
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_noalloc_rhs_3d_and_gravity(strict):
+    """Two more calls in a row: a 3D grid with mirror and outlet sides (three
+    directions of line ends in the one scratch table), then the 2D gravity
+    source with mirror walls in x and y."""
+    from cfd_inwsl_b200 import zone
+    from tests.util import make_info, smooth_state_3d
+    rng = np.random.default_rng(77)
+    n3 = [16, 12, 10]
+    c3 = smooth_state_3d(n3, rng)
+    bc3 = [[zone.BndType.SYMMETRYX, zone.BndType.SUPERSONICOUTLET],
+           [zone.BndType.SUPERSONICOUTLET, zone.BndType.SYMMETRYY],
+           [zone.BndType.SYMMETRYZ, zone.BndType.PERIODIC1D]]
+    s3 = gpu_solver(3, n3, im=11, fm=0, strict=strict, bc=bc3)
+    s3.set_cons(c3)
+    want3 = s3.rhsSolve()
+    got3 = _noalloc_rhs(s3, c3)
+    info = make_info(2, [40, 24], [0, 1, 0, 0.6, 0, 0], im=2, fm=1, strict=strict)
+    info.sourceType = zone.SourceType.GRAVITY
+    s2 = zone.BlockSolver(info, bc=[[zone.BndType.SYMMETRYX] * 2, [zone.BndType.SYMMETRYY] * 2, [7, 7]])
+    prim = np.column_stack([rng.uniform(0.5, 2, 960), rng.uniform(-1, 1, (960, 2)), rng.uniform(0.5, 2, 960)])
+    c2 = zone.prim_to_cons(prim)
+    s2.set_cons(c2)
+    want2 = s2.rhsSolve()
+    got2 = _noalloc_rhs(s2, c2)
+    for got, want in ((got3, want3), (got2, want2)):
+        assert np.all(np.isfinite(got))
+        if strict:
+            np.testing.assert_array_equal(got, want)
+        else:
+            assert rel_linf(got, want) < 1e-12
+    s3.close()
+    s2.close()
