@@ -49,6 +49,7 @@ class CfdConfig(C.Structure):
         ("device", C.c_int),
         ("seg_len", C.c_int * 3),
         ("source_type", C.c_int),
+        ("positivity", C.c_int),
     ]
 
 
@@ -74,6 +75,8 @@ _PROTOS = {
                                    C.POINTER(C.c_void_p)]),
     "cfd_set_state_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cfd_eval_inter5": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "cfd_check_division": (C.c_int, [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_ulonglong)]),
+    "cfd_fp64_peak_probe": (C.c_int, [C.c_longlong, C.c_void_p, C.POINTER(C.c_double)]),
     "cfd_eval_flux": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "cfd_version": (C.c_char_p, []),
     "cfd_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
@@ -93,6 +96,7 @@ _PROTOS = {
     "cfd_rhs_noalloc": (C.c_int, [C.POINTER(CfdConfig), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     "cfd_rhs_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "cfd_adjoint_record": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
+    "cfd_run_fixed": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
     "cfd_adjoint_reverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "cfd_enable_halo": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
     "cfd_stage_state": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),

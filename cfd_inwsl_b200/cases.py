@@ -47,14 +47,35 @@ def tgv_state(n):
     return prim_to_cons(prim), h
 
 
+def quadrant_prims(rng):
+    """The four quadrant states (rho, u, v, p) of one seeded Riemann problem:
+    rho ~ U[0.1,2], u, v ~ U[-1,1], p ~ U[0.05,2] (quadrants in the order
+    lower-left, lower-right, upper-left, upper-right)."""
+    return np.array([[rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.05, 2)]
+                     for _ in range(4)])
+
+
+def quadrant_state(P, n):
+    """Cell-centred cons (n*n, 4) of the quadrant states P on [0,1]^2 split at (0.5, 0.5)."""
+    X, Y = np.meshgrid((np.arange(n) + 0.5) / n, (np.arange(n) + 0.5) / n)
+    q = (X >= 0.5).astype(int) + 2 * (Y >= 0.5).astype(int)
+    return prim_to_cons(np.asarray(P)[q].reshape(-1, 4))
+
+
 def riemann_quadrants(n, rng):
     """Four-quadrant 2D Riemann state on [0,1]^2 split at (0.5, 0.5): each
     quadrant's rho ~ U[0.1,2], u, v ~ U[-1,1], p ~ U[0.05,2]."""
-    P = np.array([[rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.05, 2)]
-                  for _ in range(4)])
-    X, Y = np.meshgrid((np.arange(n) + 0.5) / n, (np.arange(n) + 0.5) / n)
-    q = (X >= 0.5).astype(int) + 2 * (Y >= 0.5).astype(int)
-    return prim_to_cons(P[q].reshape(-1, 4))
+    return quadrant_state(quadrant_prims(rng), n)
+
+
+def riemann_batch(ncases=256, seed=0):
+    """The batched configuration's cases: grid sizes N = round(2^U(7,10)) and
+    quadrant states, drawn in this order from one seeded generator (sizes
+    first, then each case's four states). Returns (sizes, prims)."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(round(2 ** rng.uniform(7, 10))) for _ in range(ncases)]
+    prims = [quadrant_prims(rng) for _ in sizes]
+    return sizes, prims
 
 
 def adjoint_problem(n=256, seed=0, nprobe=64):

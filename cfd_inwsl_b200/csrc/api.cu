@@ -125,6 +125,85 @@ __global__ void step_end_kernel(cfd::StepCtl *c, const unsigned long long *red, 
     c->k++;
 }
 
+// FP64 peak probe: eight independent DFMA chains per thread over every SM,
+// the denominator of the FP64 roofline (measured on the device that runs the
+// sweeps instead of a datasheet figure).
+__device__ double g_dfma_sink;
+
+__global__ void dfma_probe_kernel(long long iters, double seed)
+{
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) x[i] = seed + threadIdx.x * 1e-9 + i * 1e-3;
+    const double a = 0.999999999, b = 1e-9;
+    for (long long it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = fma(x[i], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += x[i];
+    if (s == -1.0) g_dfma_sink = s;  // never true: keeps the chains live
+}
+
+// Self-check of the strict flavour's shared-reciprocal division (div_rn)
+// against the device's IEEE division, bit for bit, on n seeded operand pairs:
+// random significands and exponents, quotients constructed next to a rounding
+// midpoint (a = RN(b (q + ulp(q)/2))), physical ranges, zeros of both signs
+// and tiny dividends.
+__device__ unsigned long long splitmix64(unsigned long long &x)
+{
+    unsigned long long z = (x += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__device__ double rand_double(unsigned long long &st, int emin, int emax)
+{
+    const unsigned long long r = splitmix64(st);
+    const int e = emin + (int)(splitmix64(st) % (unsigned long long)(emax - emin + 1));
+    const unsigned long long bits = ((unsigned long long)(1023 + e) << 52) | (r & ((1ULL << 52) - 1));
+    return __longlong_as_double((long long)bits) * ((r >> 63) ? -1.0 : 1.0);
+}
+
+__global__ void division_check_kernel(long long n, unsigned long long seed, unsigned long long *bad)
+{
+    unsigned long long cnt = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long st = seed ^ ((unsigned long long)i * 0xD1B54A32D192ED03ULL);
+        double a, b;
+        switch (i % 4) {
+        case 0:
+            a = rand_double(st, -60, 60);
+            b = fabs(rand_double(st, -60, 60));
+            break;
+        case 1: {  // the quotient next to a midpoint between two doubles
+            b = fabs(rand_double(st, -20, 20));
+            const double q = fabs(rand_double(st, -20, 20));
+            const double half_ulp = ldexp(1.0, ilogb(q) - 53);
+            a = fma(b, q, b * half_ulp);
+            break;
+        }
+        case 2:  // densities, sound speeds, enthalpies over momenta, energies, velocities
+            a = rand_double(st, -30, 12);
+            b = fabs(rand_double(st, -10, 10));
+            break;
+        default: {  // zeros, tiny and huge dividends (IEEE fallback)
+            const unsigned long long k = splitmix64(st) % 4;
+            a = (k == 0) ? 0.0 : (k == 1) ? -0.0 : (k == 2) ? rand_double(st, -1010, -950) : rand_double(st, 950, 1000);
+            b = fabs(rand_double(st, -5, 5));
+            break;
+        }
+        }
+        const double y = cfd::rcp_rn(b);
+        const double got = cfd::div_rn(a, b, y), want = a / b;
+        if (__double_as_longlong(got) != __double_as_longlong(want) || __double_as_longlong(y) != __double_as_longlong(1.0 / b))
+            cnt++;
+    }
+    if (cnt) atomicAdd(bad, cnt);
+}
+
 // Pointwise test kernels.
 template <int FAM>
 __global__ void eval_inter5_kernel(const double *q, int n, double c, double kap, double *out)
@@ -481,6 +560,7 @@ SweepParams base_params(cfd_handle *h, int d)
     p.halo_hi = h->halo[1];
     p.halo_nl = h->ncell / h->cfg.n[h->dim - 1];
     p.diff = h->cfg.diff_method;
+    p.posl = h->cfg.positivity;
     return p;
 }
 
@@ -697,6 +777,8 @@ int cfd_create(const cfd_config *cfg, cfd_handle **out)
     if (cfg->precision == CFD_PREC_MIXED && map_inter_method(cfg->inter_method, cfg->dim).fam == cfd::FAM_RESEARCH)
         return CFD_ERR_UNSUPPORTED;  // the research variants have no FP32 decision form
     if (cfg->source_type != 0 && !(cfg->source_type == 1 && cfg->dim == 2)) return CFD_ERR_UNSUPPORTED;
+    if (cfg->positivity != 0 && cfg->positivity != 1) return CFD_ERR_CONFIG;
+    if (cfg->positivity && cfg->precision == CFD_PREC_MIXED) return CFD_ERR_UNSUPPORTED;  // FP64 faces only
     for (int d = 0; d < 3; d++) {
         if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
         if (d >= cfg->dim && cfg->n[d] != 1) return CFD_ERR_CONFIG;
@@ -1030,6 +1112,31 @@ int cfd_set_state_device(cfd_handle *h, const double *soa_dev)
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));
     h->ws_valid = false;
     return CFD_OK;
+}
+
+int cfd_fp64_peak_probe(long long iters, void *stream, double *flops)
+{
+    if (iters < 1 || !flops) return CFD_ERR_CONFIG;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return CFD_ERR_CUDA;
+    const int blocks = sms * 8, threads = 256;
+    dfma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, 1.0);
+    if (cudaGetLastError() != cudaSuccess) return CFD_ERR_CUDA;
+    *flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+    return CFD_OK;
+}
+
+int cfd_check_division(long long n, unsigned long long seed, unsigned long long *mismatches)
+{
+    if (n < 0 || !mismatches) return CFD_ERR_CONFIG;
+    unsigned long long *d = nullptr;
+    if (cudaMalloc(&d, sizeof(unsigned long long)) != cudaSuccess) return CFD_ERR_NOMEM;
+    cudaMemset(d, 0, sizeof(unsigned long long));
+    division_check_kernel<<<148 * 8, 256>>>(n, seed, d);
+    cudaError_t e = cudaMemcpy(mismatches, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? CFD_OK : CFD_ERR_CUDA;
 }
 
 int cfd_eval_inter5(int inter_method, int strict, const double *q, int n, double *out)
@@ -1712,9 +1819,10 @@ int adjoint_supported(cfd_handle *h)
 {
     const bool fam_ok = h->fam == cfd::FAM_WCNS5 || h->fam == cfd::FAM_TENOZ || h->fam == cfd::FAM_TENOCONG;
     if (h->dim != 2 || !fam_ok || h->cfg.flux_method != CFD_FLUX_ROE || h->cfg.precision != CFD_PREC_FP64 ||
-        h->cfg.source_type != 0 || h->cfg.diff_method != CFD_DIFF_MND6)
+        h->cfg.source_type != 0 || h->cfg.diff_method != CFD_DIFF_MND6 || h->cfg.positivity != 0)
         return fail(h, CFD_ERR_UNSUPPORTED,
-                    "the adjoint covers 2D WCNS5 / TENO-Z / TENO-Cong + Roe + MND6, FP64, without source terms");
+                    "the adjoint covers 2D WCNS5 / TENO-Z / TENO-Cong + Roe + MND6, FP64, without source terms "
+                    "or the positivity option");
     for (int d = 0; d < 2; d++)
         for (int sd = 0; sd < 2; sd++)
             if (h->cfg.bc[d][sd] != CFD_BND_PERIODIC_WRAP)
@@ -1844,6 +1952,55 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
     h->adj_dt = dt;
     h->adj_nsteps = nsteps;
     h->adj_every = ckpt_every;
+    unsigned err = 0;
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+    CFD_CUDA(h, cudaStreamSynchronize(h->stream));
+    return check_err(h, err);
+}
+
+int cfd_run_fixed(cfd_handle *h, double dt, int nsteps, int steps_per_graph)
+{
+    if (!h || nsteps < 0 || !(dt > 0.0) || steps_per_graph < 1) return CFD_ERR_CONFIG;
+    // the stage times stay at 0: refuse boundaries that depend on time
+    for (int d = 0; d < h->dim; d++)
+        for (const auto *tab : {&h->bc_lo[d], &h->bc_hi[d]})
+            for (const BcLine &b : *tab)
+                if (b.type == cfd::BND_DOUBLEMACHUP)
+                    return fail(h, CFD_ERR_UNSUPPORTED, "cfd_run_fixed: a DoubleMachUp boundary depends on time");
+    int rc;
+    if ((rc = sync_bc(h))) return rc;
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
+    // the K-step graphs are those of cfd_adjoint_record (the same steps)
+    const int K = steps_per_graph;
+    if (h->adj_graph_K != K || h->adj_graph_dt != dt) {
+        drop_graphs(h);
+        h->adj_graph_K = K;
+        h->adj_graph_dt = dt;
+    }
+    auto steps_from = [&](int slot, int cnt) -> int {
+        for (int j = 0; j < cnt; j++) {
+            const int c = (slot + j) % 3;
+            double *S[3] = {h->u[c], h->u[(c + 1) % 3], h->u[(c + 2) % 3]};
+            int r = adjoint_step(h, dt, S, S[1]);
+            if (r) return r;
+        }
+        return CFD_OK;
+    };
+    for (int s0 = 0; s0 < nsteps; s0 += K) {
+        const int cnt = std::min(K, nsteps - s0);
+        if (cnt == K) {
+            const int slot = h->cur;
+            if (!h->adj_rec_graph[slot] &&
+                (rc = capture_graph(h, [&] { return steps_from(slot, K); }, &h->adj_rec_graph[slot])))
+                return rc;
+            CFD_CUDA(h, cudaGraphLaunch(h->adj_rec_graph[slot], h->stream));
+            h->launches += 3ULL * h->dim * K;
+        } else if ((rc = steps_from(h->cur, cnt))) {
+            return rc;
+        }
+        h->cur = (h->cur + cnt) % 3;
+    }
+    h->ws_valid = false;
     unsigned err = 0;
     CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -29,6 +29,59 @@ constexpr double kGamma = 1.4;
 constexpr double kG1 = kGamma / (kGamma - 1);   // gamma / (gamma - 1)
 constexpr double kInvGm1 = 1.0 / (kGamma - 1);  // 1 / (gamma - 1)
 #endif
+constexpr double kGm1 = kGamma - 1;             // gamma - 1 as the reference rounds it
+constexpr double kRcpGm1 = 1.0 / kGm1;          // RN(1 / (gamma - 1))
+
+// ---------------------------------------------------------------------------
+// Correctly rounded division by a shared reciprocal (strict flavour).
+//
+// The strict flavour must round every quotient exactly as an IEEE division
+// does. Where several numerators share one denominator b, y = RN(1/b) is formed
+// once and each quotient is derived from it with Markstein's correction
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990, and the FMA-based
+// division proofs of Cornea-Hasegan, Golliver and Markstein, 1999): if q is
+// within one ulp of a/b and y = RN(1/b), the residual r = a - b q is exact in
+// an FMA and RN(q + r y) = RN(a/b). q0 = RN(a y) can lie slightly more than
+// one ulp away, so a first correction brings it within a small fraction of an
+// ulp and a second applies the theorem: five FP64 operations against about
+// thirteen FP64 issue slots for a division on B200 (measured). Dividends that
+// are zero, tiny (below 2^-960, where the residual could be subnormal), huge
+// or not finite take the IEEE division itself, so zeros keep their sign. The
+// denominators here are densities, sound speeds, enthalpies and spacings,
+// normal numbers far from the ends of the exponent range.
+// ---------------------------------------------------------------------------
+CFD_HD double rcp_rn(double b)
+{
+#if defined(__CUDA_ARCH__)
+    return __drcp_rn(b);
+#else
+    return 1.0 / b;
+#endif
+}
+
+#if defined(__CUDACC__)
+// The IEEE division itself, out of line: the rare operands of div_rn take it,
+// and keeping its inline expansion out of every call site keeps the sweep's
+// instruction footprint small.
+static __device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
+#endif
+
+CFD_HD double div_rn(double a, double b, double y)
+{
+#if defined(__CUDA_ARCH__)
+    const double aa = fabs(a);
+    if (!(aa >= 0x1p-960 && aa <= 0x1p960)) return div_ieee(a, b);
+    double q = a * y;
+    double r = fma(-b, q, a);
+    q = fma(r, y, q);
+    r = fma(-b, q, a);
+    return fma(r, y, q);
+#else
+    (void)y;
+    return a / b;
+#endif
+}
 
 // ---------------------------------------------------------------------------
 // Five-point interpolators (zone_FD/src/include/interScheme.hpp).
@@ -41,6 +94,22 @@ constexpr double kInvGm1 = 1.0 / (kGamma - 1);  // 1 / (gamma - 1)
 CFD_HD void smoothness3(double q0, double q1, double q2, double q3, double q4,
                         double &b0, double &b1, double &b2)
 {
+#if defined(__CUDA_ARCH__) && !defined(CFD_FAST)
+    // The same roundings with fewer instructions: a product by a power of two
+    // is exact, so x - 2 y, x - 4 y and x + 0.25 y each round once whether
+    // they are fused or not; 0.0 * q2 adds a signed zero, which changes no
+    // finite sum (and b1 only enters squared).
+    double a, b;
+    a = fma(-2.0, q1, q0) + q2;
+    b = fma(-4.0, q1, q0) + 3.0 * q2;
+    b0 = fma(0.25, b * b, a * a);
+    a = fma(-2.0, q2, q1) + q3;
+    b = q1 - q3;
+    b1 = fma(0.25, b * b, a * a);
+    a = fma(-2.0, q3, q2) + q4;
+    b = fma(-4.0, q3, 3.0 * q2) + q4;
+    b2 = fma(0.25, b * b, a * a);
+#else
     double a, b;
     a = 1.0 * q0 - 2.0 * q1 + 1.0 * q2;
     b = 1.0 * q0 - 4.0 * q1 + 3.0 * q2;
@@ -51,6 +120,7 @@ CFD_HD void smoothness3(double q0, double q1, double q2, double q3, double q4,
     a = 1.0 * q2 - 2.0 * q3 + 1.0 * q4;
     b = 3.0 * q2 - 4.0 * q3 + 1.0 * q4;
     b2 = 1.0 / 1.0 * (a * a) + 1.0 / 4.0 * (b * b);
+#endif
 }
 
 // The three third-order candidate values (interScheme.hpp:31-33).
@@ -425,7 +495,8 @@ CFD_HD double inter5(double q0, double q1, double q2, double q3, double q4, doub
         return (w0 * u0 + w1 * u1 + w2 * u2) / (w0 + w1 + w2);
 #else
         double s;
-        s = eps + b0; b0 = (1.0 / 16.0) / (s * s);
+        // (1/16) / s^2 = RN(1 / s^2) / 16 exactly (a power-of-two scaling)
+        s = eps + b0; b0 = rcp_rn(s * s) * (1.0 / 16.0);
         s = eps + b1; b1 = (5.0 / 8.0) / (s * s);
         s = eps + b2; b2 = (5.0 / 16.0) / (s * s);
         double sumbeta = 0.0, result = 0.0;
@@ -510,8 +581,9 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         double u = ru * ir;
         double E = rE * ir;
 #else
-        double u = ru / r;
-        double E = rE / r;
+        const double ir = rcp_rn(r);
+        double u = div_rn(ru, r, ir);
+        double E = div_rn(rE, r, ir);
 #endif
         double e = -u * u / 2 + E;
         double RT = (gamma - 1) * e;
@@ -522,7 +594,8 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         const double ir = 1.0 / r;
         double u = ru * ir, v = rv * ir, E = rE * ir;
 #else
-        double u = ru / r, v = rv / r, E = rE / r;
+        const double ir = rcp_rn(r);
+        double u = div_rn(ru, r, ir), v = div_rn(rv, r, ir), E = div_rn(rE, r, ir);
 #endif
         double q2 = (u * u + v * v) / 2;
         double e = -q2 + E;
@@ -534,7 +607,8 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         const double ir = 1.0 / r;
         double u = ru * ir, v = rv * ir, w = rw * ir, E = rE * ir;
 #else
-        double u = ru / r, v = rv / r, w = rw / r, E = rE / r;
+        const double ir = rcp_rn(r);
+        double u = div_rn(ru, r, ir), v = div_rn(rv, r, ir), w = div_rn(rw, r, ir), E = div_rn(rE, r, ir);
 #endif
         double q2 = (u * u + v * v + w * w) / 2;
         double e = -q2 + E;
@@ -555,7 +629,7 @@ CFD_HD void prim_to_cons(const double *p, double *c)
 #if defined(CFD_FAST)
         c[0] = rt; c[1] = rt * ut; c[2] = pt * kInvGm1 + rt * ekt;
 #else
-        c[0] = rt; c[1] = rt * ut; c[2] = pt / (gamma - 1) + rt * ekt;
+        c[0] = rt; c[1] = rt * ut; c[2] = div_rn(pt, kGm1, kRcpGm1) + rt * ekt;
 #endif
     } else if constexpr (NV == 4) {
         double rt = p[0], ut = p[1], vt = p[2], pt = p[3];
@@ -563,7 +637,7 @@ CFD_HD void prim_to_cons(const double *p, double *c)
 #if defined(CFD_FAST)
         c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = pt * kInvGm1 + rt * ekt;
 #else
-        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = pt / (gamma - 1) + rt * ekt;
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = div_rn(pt, kGm1, kRcpGm1) + rt * ekt;
 #endif
     } else {
         double rt = p[0], ut = p[1], vt = p[2], wt = p[3], pt = p[4];
@@ -571,7 +645,7 @@ CFD_HD void prim_to_cons(const double *p, double *c)
 #if defined(CFD_FAST)
         c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = pt * kInvGm1 + rt * ekt;
 #else
-        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = pt / (gamma - 1) + rt * ekt;
+        c[0] = rt; c[1] = rt * ut; c[2] = rt * vt; c[3] = rt * wt; c[4] = div_rn(pt, kGm1, kRcpGm1) + rt * ekt;
 #endif
     }
 }
@@ -776,8 +850,9 @@ CFD_HD void char_cons_to_prim(const double *cs, double *p)
         double ut = rut * irt, vt = rvt * irt;
         double rekt = (rut * rut + rvt * rvt) * (0.5 * irt);
 #else
-        double ut = rut / rt, vt = rvt / rt;
-        double rekt = (rut * rut + rvt * rvt) / rt / 2;
+        const double irt = rcp_rn(rt);
+        double ut = div_rn(rut, rt, irt), vt = div_rn(rvt, rt, irt);
+        double rekt = div_rn(rut * rut + rvt * rvt, rt, irt) / 2;
 #endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = (gamma - 1) * (ret - rekt);
     } else {
@@ -787,8 +862,9 @@ CFD_HD void char_cons_to_prim(const double *cs, double *p)
         double ut = rut * irt, vt = rvt * irt, wt = rwt * irt;
         double rekt = (rut * rut + rvt * rvt + rwt * rwt) * (0.5 * irt);
 #else
-        double ut = rut / rt, vt = rvt / rt, wt = rwt / rt;
-        double rekt = (rut * rut + rvt * rvt + rwt * rwt) / rt / 2;
+        const double irt = rcp_rn(rt);
+        double ut = div_rn(rut, rt, irt), vt = div_rn(rvt, rt, irt), wt = div_rn(rwt, rt, irt);
+        double rekt = div_rn(rut * rut + rvt * rvt + rwt * rwt, rt, irt) / 2;
 #endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = wt; p[4] = (gamma - 1) * (ret - rekt);
     }
@@ -817,6 +893,41 @@ CFD_HD void positive_limit_1d(int which, const double *W, double *Wi)
     }
     double theta = (EPS - q) / (qi - q);
     for (int i = 0; i < 3; i++) Wi[i] = (1 - theta) * W[i] + theta * Wi[i];
+}
+
+// variable_positive_limiter (positive_preserving.hpp:13-46) on a 2D/3D cons
+// state, the option cfd_config.positivity: which = 0 limits the density,
+// which = 1 gamma p with p = (gamma - 1) (rho E - rho |u|^2 / 2), u = (rho u) / rho
+// by component. This extends the 1D quantity of reconstructor5order.hpp:210-223
+// to the multi-dimensional kinetic energy; the reference itself limits only
+// in 1D.
+template <int NV>
+CFD_HD double positive_quantity_md(int which, const double *W)
+{
+    if (which == 0) return W[0];
+    const double rho = W[0];
+    double q2 = 0.0;
+    for (int i = 1; i < NV - 1; i++) {
+        const double u = W[i] / rho;
+        q2 = q2 + u * u;
+    }
+    const double ekin = 0.5 * q2;
+    const double p = (kGamma - 1) * (W[NV - 1] - rho * ekin);
+    return kGamma * p;
+}
+template <int NV>
+CFD_HD void positive_limit_md(int which, const double *W, double *Wi)
+{
+    const double EPS = 1e-10;
+    const double qi = positive_quantity_md<NV>(which, Wi);
+    if (qi >= EPS) return;
+    const double q = positive_quantity_md<NV>(which, W);
+    if (q < EPS) {
+        for (int i = 0; i < NV; i++) Wi[i] = W[i];
+        return;
+    }
+    const double theta = (EPS - q) / (qi - q);
+    for (int i = 0; i < NV; i++) Wi[i] = (1 - theta) * W[i] + theta * Wi[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -878,8 +989,11 @@ CFD_HD void reconstruct_face(const double (*pr6)[NV], const double (*cs6)[NV], d
 template <int NV, int AX>
 struct EigenBase {
     double u, v, w, h, c, ek, Vn;
-#if defined(CFD_FAST)
-    double ic, ih;
+    double ic, ih;  // 1/c and 1/h (strict: RN(1/c), RN(1/h))
+#if !defined(CFD_FAST)
+    // strict: the correctly rounded quotients the eigenvectors use, each formed
+    // once per face (Vn/c, ek/h, u/h, v/h, w/h)
+    double Vc, ekh, uh, vh, wh;
 #endif
     static constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0, nz = (AX == 2) ? 1.0 : 0.0;
 
@@ -887,24 +1001,55 @@ struct EigenBase {
     template <class PR>
     CFD_HD EigenBase(const PR &pr)
     {
+        double pl[NV], prr[NV], kl[NV], kr[NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+            pl[m] = pr(2, m);
+            prr[m] = pr(3, m);
+        }
+        roe_weights(pl, kl);
+        roe_weights(prr, kr);
+        init(kl, kr);
+    }
+    // from the two cells' Roe weights (roe_weights), e.g. kept per cell by the sweep
+    CFD_HD EigenBase(const double *kl, const double *kr) { init(kl, kr); }
+
+    // A cell's share of the Roe average: (sqrt(rho), sqrt(rho) u, sqrt(rho) v,
+    // [sqrt(rho) w,] sqrt(rho) H), each product rounded as the reference's
+    // coef * v and coef * H are (eigenSystem.cpp:17-30); H = |v|^2 / 2 +
+    // p / rho * gamma / (gamma - 1).
+    static CFD_HD void roe_weights(const double *p, double *k)
+    {
+        constexpr int D = NV - 2, E = NV - 1;
+        const double r = p[0], pp = p[E];
+        double q2 = p[1] * p[1] + p[2] * p[2];
+        if constexpr (D == 3) q2 = q2 + p[3] * p[3];
+#if defined(CFD_FAST)
+        // sqrt(rho) = rho rsqrt(rho), sqrt(rho) H = sqrt(rho) |v|^2 / 2 +
+        // gamma/(gamma-1) p rsqrt(rho)
+        const double ir = rsqrt(r);
+        const double coef = r * ir;
+        k[E] = 0.5 * (coef * q2) + kG1 * (pp * ir);
+#else
+        const double coef = sqrt(r);
+        const double H = q2 / 2 + div_rn(pp / r * kGamma, kGm1, kRcpGm1);
+        k[E] = coef * H;
+#endif
+        k[0] = coef;
+#pragma unroll
+        for (int i = 0; i < D; i++) k[1 + i] = coef * p[1 + i];
+    }
+
+  private:
+    CFD_HD void init(const double *kl, const double *kr)
+    {
         constexpr int D = NV - 2;
         const double gamma = kGamma;
-        double vl[3] = {pr(2, 1), pr(2, 2), D == 3 ? pr(2, 3) : 0.0};
-        double vr[3] = {pr(3, 1), pr(3, 2), D == 3 ? pr(3, 3) : 0.0};
-        double rl = pr(2, 0), rr = pr(3, 0), pL = pr(2, NV - 1), pR = pr(3, NV - 1);
-#if defined(CFD_FAST)
-        // reciprocal square roots replace the divisions: sqrt(rho) = rho rsqrt(rho),
-        // sqrt(rho) H = sqrt(rho) |v|^2 / 2 + gamma/(gamma-1) p rsqrt(rho),
-        // 1/c = rsqrt(c^2), 1/h = (gamma - 1) / c^2
-        double kl = vl[0] * vl[0] + vl[1] * vl[1], kr = vr[0] * vr[0] + vr[1] * vr[1];
-        if constexpr (D == 3) { kl += vl[2] * vl[2]; kr += vr[2] * vr[2]; }
-        const double ir1 = rsqrt(rl), ir2 = rsqrt(rr);
-        const double coef1 = rl * ir1, coef2 = rr * ir2;
-        const double divisor = 1.0 / (coef1 + coef2);
-        u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
-        v = (coef1 * vl[1] + coef2 * vr[1]) * divisor;
-        w = (D == 3) ? (coef1 * vl[2] + coef2 * vr[2]) * divisor : 0.0;
-        const double ht = (0.5 * (coef1 * kl + coef2 * kr) + kG1 * (pL * ir1 + pR * ir2)) * divisor;
+        const double divisor = 1.0 / (kl[0] + kr[0]);
+        u = (kl[1] + kr[1]) * divisor;
+        v = (kl[2] + kr[2]) * divisor;
+        w = (D == 3) ? (kl[3] + kr[3]) * divisor : 0.0;
+        const double ht = (kl[NV - 1] + kr[NV - 1]) * divisor;
         if constexpr (D == 2) {
             Vn = nx * u + ny * v;
             ek = (u * u + v * v) / 2;
@@ -913,43 +1058,33 @@ struct EigenBase {
             ek = (u * u + v * v + w * w) / 2;
         }
         h = ht - ek;
+#if defined(CFD_FAST)
+        // 1/c = rsqrt(c^2), 1/h = (gamma - 1) / c^2
         const double c2 = (gamma - 1) * h;
         ic = rsqrt(c2);
         c = c2 * ic;
         ih = (gamma - 1) * (ic * ic);
 #else
-        double HL, HR;
-        if constexpr (D == 2) {
-            HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pL / rl * gamma / (gamma - 1);
-            HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pR / rr * gamma / (gamma - 1);
-        } else {
-            HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pL / rl * gamma / (gamma - 1);
-            HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pR / rr * gamma / (gamma - 1);
-        }
-        double coef1 = sqrt(rl), coef2 = sqrt(rr);
-        double divisor = 1.0 / (coef1 + coef2);
-        u = (coef1 * vl[0] + coef2 * vr[0]) * divisor;
-        v = (coef1 * vl[1] + coef2 * vr[1]) * divisor;
-        w = (D == 3) ? (coef1 * vl[2] + coef2 * vr[2]) * divisor : 0.0;
-        double ht = (coef1 * HL + coef2 * HR) * divisor;
-        if constexpr (D == 2) {
-            Vn = nx * u + ny * v;
-            ek = (u * u + v * v) / 2;
-        } else {
-            Vn = nx * u + ny * v + nz * w;
-            ek = (u * u + v * v + w * w) / 2;
-        }
-        h = ht - ek;
         c = sqrt((gamma - 1) * h);
+        ic = rcp_rn(c);
+        ih = rcp_rn(h);
+        Vc = div_rn(Vn, c, ic);
+        ekh = div_rn(ek, h, ih);
+        uh = div_rn(u, h, ih);
+        vh = div_rn(v, h, ih);
+        wh = (D == 3) ? div_rn(w, h, ih) : 0.0;
 #endif
     }
+
+  public:
 #if defined(CFD_FAST)
     CFD_HD double dc(double a) const { return a * ic; }
     CFD_HD double dh(double a) const { return a * ih; }
-#else
-    CFD_HD double dc(double a) const { return a / c; }
-    CFD_HD double dh(double a) const { return a / h; }
 #endif
+    // (s n_i) / c for a unit normal component n_i (0 or 1) and s = -1 or 1:
+    // the correctly rounded 1/c with the sign, or a signed zero, exactly as
+    // the division rounds it
+    CFD_HD double sn_c(double s, double n) const { return (s * n) * ic; }
     // left eigenvector k, column m (eigenSystem.cpp:53-68 and the 3D extension)
     CFD_HD double L(int k, int m) const
     {
@@ -961,17 +1096,20 @@ struct EigenBase {
         if (k == 1) return m == 0 ? (h - ek) : m == 1 ? u : m == 2 ? v : m == E ? -1.0 : w;
         if (k == 2 || k == 3) {
             const double s = (k == 2) ? -1.0 : 1.0;
-            if (m == E) {
+            // 1 / (2 h) = RN(1/h) / 2 exactly
+            if (m == E) return 0.5 * ih;
 #if defined(CFD_FAST)
-                return 0.5 * ih;
-#else
-                return 1.0 / (2.0 * h);
-#endif
-            }
             if (m == 0) return (k == 2) ? (dc(Vn) + dh(ek)) / 2 : (dc(-Vn) + dh(ek)) / 2;
             if (m == 1) return (dc(s * nx) - dh(u)) / 2;
             if (m == 2) return (dc(s * ny) - dh(v)) / 2;
             return (dc(s * nz) - dh(w)) / 2;
+#else
+            // (-Vn) / c = -(Vn / c) exactly
+            if (m == 0) return (k == 2) ? (Vc + ekh) / 2 : (-Vc + ekh) / 2;
+            if (m == 1) return (sn_c(s, nx) - uh) / 2;
+            if (m == 2) return (sn_c(s, ny) - vh) / 2;
+            return (sn_c(s, nz) - wh) / 2;
+#endif
         }
         // k == 4: second shear wave (3D only)
         if (AX != 2) return m == 0 ? -w : m == 3 ? 1.0 : 0.0;
@@ -985,7 +1123,11 @@ struct EigenBase {
             if (AX != 2) return i == 0 ? 0.0 : i == 1 ? ny : i == 2 ? -nx : i == E ? ny * u - nx * v : 0.0;
             return i == 1 ? 1.0 : i == E ? u : 0.0;
         }
+#if defined(CFD_FAST)
         if (k == 1) return i == 0 ? dh(1.0) : i == 1 ? dh(u) : i == 2 ? dh(v) : i == E ? dh(ek) : dh(w);
+#else
+        if (k == 1) return i == 0 ? ih : i == 1 ? uh : i == 2 ? vh : i == E ? ekh : wh;
+#endif
         if (k == 2 || k == 3) {
             const double s = (k == 2) ? -1.0 : 1.0;
             if (i == 0) return 1.0;
@@ -1000,12 +1142,14 @@ struct EigenBase {
     }
 };
 
-// cs(j, v): re-derived cons of stencil cell j (0..5), pr(j, v): its prim.
+// cs(j, v): re-derived cons of stencil cell j (0..5), pr(j, v): its prim;
+// eb: the face's Roe-averaged eigensystem; posl: the positivity option
+// (cfd_config.positivity) instead of the reference's fallback.
 template <int NV, int AX, int FAM, class CS, class PR>
-CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, double kap, double *fl, double *fr)
+CFD_HD void reconstruct_face_stream(const EigenBase<NV, AX> &eb, const CS &cs, const PR &pr, double icst, double kap,
+                                    double *fl, double *fr, int posl = 0)
 {
     static_assert(NV == 4 || NV == 5, "multi-dimensional form");
-    const EigenBase<NV, AX> eb(pr);
     double cl[NV], cr[NV];
     // Fully unrolled: the instruction-level parallelism across fields beats the
     // smaller code of a rolled loop (measured on B200: 22.0 vs 31.9 ms per 3D
@@ -1055,6 +1199,23 @@ CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, dou
             }
         }
     }
+    if (posl) {
+        // the 1D char-recon limiter (reconstructor5order.hpp:225-236): density
+        // of both states, then gamma p of both, against the cells' cons
+        double WL[NV], WR[NV];
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            WL[i] = cs(2, i);
+            WR[i] = cs(3, i);
+        }
+        positive_limit_md<NV>(0, WL, cl);
+        positive_limit_md<NV>(0, WR, cr);
+        positive_limit_md<NV>(1, WL, cl);
+        positive_limit_md<NV>(1, WR, cr);
+        char_cons_to_prim<NV>(cl, fl);
+        char_cons_to_prim<NV>(cr, fr);
+        return;
+    }
     char_cons_to_prim<NV>(cl, fl);
     char_cons_to_prim<NV>(cr, fr);
     // crude positivity fallback (reconstructor5order.hpp:380-381), including
@@ -1067,6 +1228,15 @@ CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, dou
         for (int i = 1; i < NV - 1; i++) fr[i] = pr(2, i);
         fr[NV - 1] = pr(3, NV - 1);
     }
+}
+
+// The same with the eigensystem formed from the prim of stencil cells 2 and 3.
+template <int NV, int AX, int FAM, class CS, class PR>
+CFD_HD void reconstruct_face_stream(const CS &cs, const PR &pr, double icst, double kap, double *fl, double *fr,
+                                    int posl = 0)
+{
+    const EigenBase<NV, AX> eb(pr);
+    reconstruct_face_stream<NV, AX, FAM>(eb, cs, pr, icst, kap, fl, fr, posl);
 }
 
 // ---------------------------------------------------------------------------
@@ -1159,15 +1329,17 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
     double VnL = vl[AX], VnR = vr[AX];
     double cl = sqrt(prl * gamma), cr = sqrt(prr * gamma);
 #else
+    const double prl = pl / rl, prr = pr / rr;
+    // x / (gamma - 1) by its correctly rounded reciprocal (div_rn)
     if constexpr (D == 2) {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
+        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + div_rn(prl * kGamma, kGm1, kRcpGm1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + div_rn(prr * kGamma, kGm1, kRcpGm1);
     } else {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
+        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + div_rn(prl * kGamma, kGm1, kRcpGm1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + div_rn(prr * kGamma, kGm1, kRcpGm1);
     }
     double VnL = vl[AX], VnR = vr[AX];
-    double cl = sqrt(pl / rl * gamma), cr = sqrt(pr / rr * gamma);
+    double cl = sqrt(prl * gamma), cr = sqrt(prr * gamma);
 #endif
     double rBar = (rl + rr) / 2, cBar = (cl + cr) / 2;
     double ps0 = (pl + pr) / 2 - rBar * cBar * (VnR - VnL) / 2;
@@ -1195,21 +1367,30 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
         Ustar[E] = Usf * (U[E] + (Sstar - Vn) * (r * Sstar + p / (S - Vn)));
         for (int i = 0; i < NV; i++) {
             double f = F[i] + S * (Ustar[i] - U[i]);
-            if (scale != 1.0) f = f / 2;
-            if (accumulate) out[i] += f; else out[i] = f;
+            f = (scale != 1.0) ? f / 2 : f;
+            out[i] = accumulate ? out[i] + f : f;
         }
     };
     if (SL > 0) {
         res[0] = rl * VnL;
         for (int i = 0; i < D; i++) res[1 + i] = rl * vl[i] * VnL + pl * n[i];
         res[E] = rl * HL * VnL;
-    } else if (Sstar > 0) {
-        side_flux(rl, vl, pl, HL, VnL, SL, res, 1.0, false);
-    } else if (Sstar == 0) {
-        side_flux(rl, vl, pl, HL, VnL, SL, res, 0.5, false);
-        side_flux(rr, vr, pr, HR, VnR, SR, res, 0.5, true);
-    } else if (SR > 0) {
-        side_flux(rr, vr, pr, HR, VnR, SR, res, 1.0, false);
+    } else if (Sstar > 0 || Sstar == 0 || SR > 0) {
+        // The star-region branches of the reference in one body: S* > 0 takes
+        // the left side, S* < 0 < SR the right one, and S* = 0 the average of
+        // both halves (left first, then the right half added), so the side
+        // flux is emitted once.
+        const bool avg = (Sstar == 0);
+        const bool left = (Sstar > 0) || avg;
+#pragma unroll 1
+        for (int it = 0; it < (avg ? 2 : 1); it++) {
+            const bool useL = left && it == 0;
+            double vs[D];
+#pragma unroll
+            for (int i = 0; i < D; i++) vs[i] = useL ? vl[i] : vr[i];
+            side_flux(useL ? rl : rr, vs, useL ? pl : pr, useL ? HL : HR, useL ? VnL : VnR, useL ? SL : SR, res,
+                      avg ? 0.5 : 1.0, it > 0);
+        }
     } else {
         res[0] = rr * VnR;
         for (int i = 0; i < D; i++) res[1 + i] = rr * vr[i] * VnR + pr * n[i];
@@ -1277,6 +1458,25 @@ CFD_HD void roe_md_fast(const double *L, const double *R, double *res)
 }
 #endif
 
+// Harten's entropy fix of roeFlux2DSym (fluxSchemes.hpp:499-505): a wave speed
+// below eps becomes (lambda^2 + eps^2) / (2 eps). Out of line: few faces take
+// it, and its three divisions stay out of the sweep's instruction stream.
+struct Lam3 {
+    double a, b, c;
+};
+#if defined(__CUDACC__)
+static __host__ __device__ __noinline__
+#else
+static inline
+#endif
+Lam3 entropy_fix3(double l0, double l1, double l2, double eps)
+{
+    double l[3] = {l0, l1, l2};
+    for (int i = 0; i < 3; i++)
+        if (l[i] < eps) l[i] = (l[i] * l[i] + eps * eps) / (2.0 * eps);
+    return Lam3{l[0], l[1], l[2]};
+}
+
 // roeFlux2DSym (fluxSchemes.hpp:420-553), 3D form with both tangential
 // components in the linear wave.
 template <int NV, int AX>
@@ -1290,12 +1490,13 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
     const double *vl = L + 1, *vr = R + 1;
     double HL, HR;
+    // x / (gamma - 1) by its correctly rounded reciprocal (div_rn)
     if constexpr (D == 2) {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + pl / rl * kGamma / (kGamma - 1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + pr / rr * kGamma / (kGamma - 1);
+        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + div_rn(pl / rl * kGamma, kGm1, kRcpGm1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + div_rn(pr / rr * kGamma, kGm1, kRcpGm1);
     } else {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + pl / rl * kGamma / (kGamma - 1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + pr / rr * kGamma / (kGamma - 1);
+        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + div_rn(pl / rl * kGamma, kGm1, kRcpGm1);
+        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + div_rn(pr / rr * kGamma, kGm1, kRcpGm1);
     }
     double VnL = vl[AX], VnR = vr[AX];
     double FcL[NV], FcR[NV];
@@ -1319,24 +1520,31 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double VnAvg = vAvg[AX];
     double lambda[3] = {fabs(VnAvg - cAvg), fabs(VnAvg), fabs(VnAvg + cAvg)};
     double eps = 0.05 * (fabs(VnAvg) + cAvg);
-    for (int i = 0; i < 3; i++)
-        if (lambda[i] < eps) lambda[i] = (lambda[i] * lambda[i] + eps * eps) / (2.0 * eps);
+    if (lambda[0] < eps || lambda[1] < eps || lambda[2] < eps) {
+        const Lam3 fx = entropy_fix3(lambda[0], lambda[1], lambda[2], eps);
+        lambda[0] = fx.a;
+        lambda[1] = fx.b;
+        lambda[2] = fx.c;
+    }
 
     double deltaP = pr - pl, deltaVn = VnR - VnL, deltaRho = rr - rl;
     double dv[3];
     for (int i = 0; i < D; i++) dv[i] = vr[i] - vl[i];
     double Fd[NV];
-    double c1 = (deltaP - rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+    // the three quotients by c^2 and 2 c^2 from one correctly rounded
+    // reciprocal: (2 c) c = 2 RN(c c) exactly, so x / (2 c c) = RN(x / (c c)) / 2
+    const double cc2 = cAvg * cAvg, icc2 = rcp_rn(cc2);
+    double c1 = div_rn(deltaP - rhoAvg * cAvg * deltaVn, cc2, icc2) / 2;
     Fd[0] = lambda[0] * (c1 * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] = lambda[0] * (c1 * (vAvg[i] - cAvg * n[i]));
     Fd[E] = lambda[0] * (c1 * (HAvg - cAvg * VnAvg));
 
-    double cc = (deltaP + rhoAvg * cAvg * deltaVn) / (2.0 * cAvg * cAvg);
+    double cc = div_rn(deltaP + rhoAvg * cAvg * deltaVn, cc2, icc2) / 2;
     Fd[0] += lambda[2] * (cc * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] += lambda[2] * (cc * (vAvg[i] + cAvg * n[i]));
     Fd[E] += lambda[2] * (cc * (HAvg + cAvg * VnAvg));
 
-    double c2 = deltaRho - deltaP / (cAvg * cAvg);
+    double c2 = deltaRho - div_rn(deltaP, cc2, icc2);
     Fd[0] += lambda[1] * (c2 * 1.0 + rhoAvg * 0.0);
     // tangential components carry rhoAvg * dv_i, the normal one 0
     // (fluxSchemes.hpp:526-528 for axis normals).
@@ -1401,8 +1609,7 @@ CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fh
     (void)h;
     return (w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3)) * inv_h;
 #else
-    (void)inv_h;
-    return (w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3)) / h;
+    return div_rn(w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3), h, inv_h);
 #endif
 }
 
@@ -1417,8 +1624,7 @@ CFD_HD double trad6(double fhm5, double fhm3, double fhm1, double fhp1, double f
     (void)h;
     return (w0 * (fhp1 - fhm1) - w1 * (fhp3 - fhm3) + w2 * (fhp5 - fhm5)) * inv_h;
 #else
-    (void)inv_h;
-    return (w0 * (fhp1 - fhm1) - w1 * (fhp3 - fhm3) + w2 * (fhp5 - fhm5)) / h;
+    return div_rn(w0 * (fhp1 - fhm1) - w1 * (fhp3 - fhm3) + w2 * (fhp5 - fhm5), h, inv_h);
 #endif
 }
 

@@ -105,6 +105,7 @@ extern "C" int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, do
         cfg->precision != CFD_PREC_FP64)
         return CFD_ERR_UNSUPPORTED;
     if (cfg->flux_method != CFD_FLUX_HLLC && cfg->flux_method != CFD_FLUX_ROE) return CFD_ERR_CONFIG;
+    if (cfg->positivity != 0 && cfg->positivity != 1) return CFD_ERR_CONFIG;
     if (cfg->source_type != 0 && !(cfg->source_type == 1 && cfg->dim == 2)) return CFD_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) {
         if (d < cfg->dim && (cfg->n[d] < 5 || !(cfg->h[d] > 0.0))) return CFD_ERR_CONFIG;
@@ -206,6 +207,7 @@ extern "C" int cfd_rhs_noalloc(const cfd_config *cfg, const double *cons_soa, do
         p.dm_u = 8.25 * std::cos(M_PI / 6);
         p.dm_v = -8.25 * std::sin(M_PI / 6);
         p.gravity = (cfg->source_type == 1 && d == cfg->dim - 1) ? 1 : 0;
+        p.posl = cfg->positivity;
         if (cfd::launch_sweep_any(cfg->strict != 0, cfg->dim + 2, fam, d, cfg->flux_method, p, st) != cudaSuccess)
             rc = CFD_ERR_CUDA;
     }

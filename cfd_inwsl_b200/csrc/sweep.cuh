@@ -133,10 +133,9 @@ struct SweepShape {
     // hi + lo from the FP32 split (within 2^-48 of the cons), which leaves room
     // for the cp.async staging below (the x sweep stages less and has room).
     static constexpr bool HL_CS = (PREC == 1 && NV == 5 && AX != 0 && FAM != FAM_RESEARCH);
-    static constexpr int SMEM_DOUBLES = (HL_CS ? 1 : 2) * NV * W * LSP + NV * W * LSF;
+    static constexpr int SMEM_DOUBLES0 = (HL_CS ? 1 : 2) * NV * W * LSP + NV * W * LSF;
     // mixed form: FP32 hi/lo split of the cons ring (exact FP32 increments)
     static constexpr int SMEM_FLOATS = PREC ? 2 * NV * W * LSP : 0;
-    static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
     // Resident CTAs per SM the launch bounds ask for: 512 threads per SM in
     // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread;
     // or three 128-thread CTAs (168 registers, fewer spills), which measured
@@ -157,7 +156,16 @@ struct SweepShape {
     // operands to stage), so it stages only the next chunk's cells.
     static constexpr int NSTG = (AX == 0 && NV >= 4) ? 1 : 4;
     static constexpr size_t SMEM_STAGE = sizeof(double) * NSTG * NV * NT;
-    static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= (MINB > 2 ? 224 / MINB : 112) * 1024;
+    static constexpr size_t SMEM_LIMIT = (size_t)(MINB > 2 ? 224 / MINB : 112) * 1024;
+    // FP64 multi-dimensional sweeps keep each cell's Roe weights (sqrt(rho),
+    // sqrt(rho) v, sqrt(rho) H) beside its prim: formed once per cell instead
+    // of once for each of the cell's two faces; where the ring fits beside the
+    // staging buffers
+    static constexpr bool RW = (PREC == 0 && NV >= 4) &&
+                               sizeof(double) * (SMEM_DOUBLES0 + NV * W * LSP) + SMEM_STAGE <= SMEM_LIMIT;
+    static constexpr int SMEM_DOUBLES = SMEM_DOUBLES0 + (RW ? NV * W * LSP : 0);
+    static constexpr size_t SMEM_RINGS = sizeof(double) * SMEM_DOUBLES + sizeof(float) * SMEM_FLOATS;
+    static constexpr bool PF = SMEM_RINGS + SMEM_STAGE <= SMEM_LIMIT;
     static constexpr bool PF_EPI = PF && NSTG == 4;
     static constexpr size_t SMEM_BYTES = SMEM_RINGS + (PF ? SMEM_STAGE : 0);
 };
@@ -172,6 +180,10 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     if (p.ctl && p.ctl->done) return;
     const double tstage = p.ctl ? p.ctl->tst[p.rk_stage] : p.t;
     const double inv_h = 1.0 / p.h;
+    // RN(1/h_d) for the correctly rounded wave-speed quotients of the epilogue
+    double inv_hdir[3] = {0.0, 0.0, 0.0};
+    if (p.mode == MODE_RK && p.want_reduce)
+        for (int d = 0; d < NV - 2; d++) inv_hdir[d] = 1.0 / p.hdir[d];
     // ring positions (R and RF are powers of two; arguments are never negative)
     auto ring = [](int x) { return (int)((unsigned)x & (unsigned)(R - 1)); };
     auto fring = [](int x) { return (int)((unsigned)x & (unsigned)(RF - 1)); };
@@ -182,6 +194,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     double *sf = SH::HL_CS ? sc : sc + NV * W * LSP;  // [NV][W][LSF] face flux
     // mixed form: [NV][W][LSP] (hi, lo) = ((float)cons, (float)(cons - hi))
     float2 *shl = reinterpret_cast<float2 *>(sf + NV * W * LSF);
+    // FP64 form: [NV][W][LSP] Roe weights of each cell (in place of the mixed form's split)
+    double *skw = sf + NV * W * LSF;
     // staging: [0] next chunk's cons, [1] rhs, [2] U^0, [3] U^k; [NV][NT] each
     double *stg = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + SH::SMEM_RINGS);
     constexpr bool PF = SH::PF, PF_EPI = SH::PF_EPI;
@@ -256,6 +270,12 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         }
         if (!have_cs) prim_to_cons<NV>(pr, cs);  // as the reference's primToChar re-derives them
         int slot = ring(P - s_begin + HG);
+        if constexpr (SH::RW) {
+            double kw[NV];
+            EigenBase<NV, AX>::roe_weights(pr, kw);
+#pragma unroll
+            for (int v = 0; v < NV; v++) skw[(v * W + l) * LSP + slot] = kw[v];
+        }
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             sp[(v * W + l) * LSP + slot] = pr[v];
@@ -303,8 +323,18 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                 } else {
                     reconstruct_face_mixed<NV, AX, FAM>(csacc, pracc, hlacc, p.icst, p.icst_k, fl, fr);
                 }
+            } else if constexpr (SH::RW) {
+                const double *kwl = skw + l * LSP;
+                double kl[NV], kr[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    kl[v] = kwl[v * W * LSP + slot[2]];
+                    kr[v] = kwl[v * W * LSP + slot[3]];
+                }
+                const EigenBase<NV, AX> eb(kl, kr);
+                reconstruct_face_stream<NV, AX, FAM>(eb, csacc, pracc, p.icst, p.icst_k, fl, fr, p.posl);
             } else {
-                reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, p.icst_k, fl, fr);
+                reconstruct_face_stream<NV, AX, FAM>(csacc, pracc, p.icst, p.icst_k, fl, fr, p.posl);
             }
         }
         if constexpr (PREC == 1 && FLUX == FLUX_ROE && NV >= 4) roe_md_mixed<NV, AX>(fl, fr, fx);
@@ -366,14 +396,24 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             load_pos(tl, c0 + HG + tp);
         }
         __syncthreads();
-        if (c0 == s_begin) {  // the FC faces before the chunk's first new one
-            for (int idx = tid; idx < FC * W; idx += NT) {
-                int l = (AX == 0) ? idx / FC : idx % W;
-                int q = (AX == 0) ? idx % FC : idx / W;
-                face(l, s_begin - FO + q);
+        {
+            // the chunk's S new faces per line, and before the segment's first
+            // chunk also the FC faces ahead of them, from one call site (the
+            // face code is emitted once)
+            const int nface = (c0 == s_begin) ? NT + FC * W : NT;
+            for (int idx = tid; idx < nface; idx += NT) {
+                int l, j;
+                if (idx < NT) {
+                    l = tl;
+                    j = c0 + HG - 2 + tp;
+                } else {
+                    const int e = idx - NT;
+                    l = (AX == 0) ? e / FC : e % W;
+                    j = s_begin - FO + ((AX == 0) ? e % FC : e / W);
+                }
+                face(l, j);
             }
         }
-        face(tl, c0 + HG - 2 + tp);
         __syncthreads();
 
         const int i = c0 + tp;
@@ -444,7 +484,8 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
                     if (!(pr[0] > 0.0) || !(pr[NV - 1] > 0.0)) err |= ERR_NEGATIVE;
                     double cs = sqrt(kGamma * pr[NV - 1] / pr[0]);
 #pragma unroll
-                    for (int d = 0; d < NV - 2; d++) red_lam[d] = fmax(red_lam[d], (cs + fabs(pr[1 + d])) / p.hdir[d]);
+                    for (int d = 0; d < NV - 2; d++)
+                        red_lam[d] = fmax(red_lam[d], div_rn(cs + fabs(pr[1 + d]), p.hdir[d], inv_hdir[d]));
                 }
             }
         }

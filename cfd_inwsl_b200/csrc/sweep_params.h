@@ -123,7 +123,7 @@ struct SweepParams {
     const double *halo_lo, *halo_hi;  // BND_HALO ghosts: [var][4 rows, ascending][line]
     long long halo_nl;                // lines per halo row
     int diff;                         // DIFF_TRAD6: ExplicitDif6 with 5 ghosts; else MND6 with 4
-    int pad_diff;
+    int posl;                         // 1: the 1D positivity limiter on 2D/3D face states (cfd_config.positivity)
 };
 
 // One batched sweep launch: the parameter blocks of every case (device array)

@@ -142,6 +142,7 @@ class Info:
         self.precision = 0      # 0: FP64, 1: mixed FP32 reconstruction / FP64 state (CFD_PREC_MIXED)
         self.device = 0
         self.seg_len = [0, 0, 0]
+        self.positivity = 0     # 1: the 1D positivity limiter on 2D/3D face states (cfd_config.positivity)
 
     def getDim(self) -> int:  # info.cpp:103-114
         return sum(1 for i in range(3) if self.iMax[i] > 2)
@@ -210,6 +211,7 @@ def make_config(info: Info, bc=None, periodic: bool = False) -> _lib.CfdConfig:
     cfg.precision = int(getattr(info, "precision", 0))
     cfg.device = int(info.device)
     cfg.source_type = int(getattr(info, "sourceType", 0))
+    cfg.positivity = int(getattr(info, "positivity", 0))
     types = bc if bc is not None else default_bc_types(info)
     if periodic:
         types = [[BndType.PERIODIC_WRAP] * 2 for _ in range(3)]

@@ -100,6 +100,12 @@ typedef struct cfd_config {
     int seg_len[3];     /* cells per CTA segment along each sweep (0 = autotuned default) */
     int source_type;    /* SourceType (macro.hpp:90): 0 none, 1 GRAVITY (2D; SourceTerm::calGravitySource,
                            sourceTerm.cpp:3-20: rhs_(rho v) -= rho, rhs_(rho E) -= rho v) */
+    int positivity;     /* face states of 2D/3D reconstruction: 0 = the reference's fallback to the cell
+                           state when rho or p < 0 (reconstructor5order.hpp:380-381); 1 = the limiter
+                           the reference applies in 1D (variable_positive_limiter,
+                           positive_preserving.hpp:13-46, on rho then gamma p, as in
+                           reconstructor5order.hpp:227-232), extended to the 2D/3D cons
+                           (FP64 only; not in the adjoint) */
 } cfd_config;
 
 typedef struct cfd_handle cfd_handle;
@@ -174,6 +180,22 @@ unsigned long long cfd_launch_count(const cfd_handle *h);
  * combined like RK stage 2 (dt = 0) into a spare state slot, as the last sweep
  * of a stage runs. The current state is not changed. */
 int cfd_sweep(cfd_handle *h, int idim, int mode, double t);
+
+/* FP64 peak probe: enqueues on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) one launch of eight independent DFMA chains of `iters`
+ * steps per thread, eight 256-thread CTAs per SM, and returns in *flops the
+ * floating-point operations it performs (2 per DFMA). Timing it with events
+ * on the same stream gives the device's FP64 throughput, the denominator of
+ * the sweeps' FP64 roofline. No counterpart in the reference. */
+int cfd_fp64_peak_probe(long long iters, void *stream, double *flops);
+
+/* Self-check of the strict flavour's correctly rounded division by a shared
+ * reciprocal (Markstein's correction) against the device's IEEE division on n
+ * seeded operand pairs (random, next to rounding midpoints, physical ranges,
+ * signed zeros, tiny and huge dividends); *mismatches counts pairs whose
+ * quotient or reciprocal bits differ. No counterpart in the reference: it
+ * backs the strict flavour's bit-for-bit parity. */
+int cfd_check_division(long long n, unsigned long long seed, unsigned long long *mismatches);
 
 /* Pointwise known-answer hooks: evaluate the device interpolator for
  * inter_method on n five-point stencils (q[5*i..5*i+4] -> out[i]), and the
@@ -260,6 +282,16 @@ int cfd_batch_autotune(cfd_batch *b, int *choice, double *ms);
 /* Sets the tiling of the sweeps along idim (1/2/3) by hand: shape 0/1,
  * segments per line (1..64), one_cta 0/1, as cfd_batch_autotune reports it. */
 int cfd_batch_set_tiling(cfd_batch *b, int idim, int shape, int segments, int one_cta);
+
+/* Frozen-dt time loop: nsteps SSP-RK3 steps of one fixed dt (no CFL step,
+ * no output clipping), replayed from captured CUDA graphs of steps_per_graph
+ * steps (the forward steps of cfd_adjoint_record, without its checkpoints).
+ * Stage times stay at 0, so time-dependent boundaries (DoubleMachUp) are
+ * refused with CFD_ERR_UNSUPPORTED. Returns after the steps finished, with
+ * CFD_ERR_NONFINITE / CFD_ERR_NEGATIVE_STATE as cfd_rk3_step. The loop the
+ * reference runs with a fixed step is BlockSolver::solve's RK3_SSP sequence
+ * (blockSolver.cpp:43-87). */
+int cfd_run_fixed(cfd_handle *h, double dt, int nsteps, int steps_per_graph);
 
 /* Discrete adjoint. The reference has no adjoint; these entry points serve
  * gradient studies of the same discretisation (sensitivity of a functional of

@@ -269,6 +269,32 @@ static void pos_limit(int which, const double *W, double *Wi)
     for (int i = 0; i < 3; i++) Wi[i] = (1 - th) * W[i] + th * Wi[i];
 }
 
+/* The positivity option on a 2D/3D cons state (the library's
+   positive_quantity_md / positive_limit_md): gamma p with
+   p = (gamma - 1) (rho E - rho |u|^2 / 2), |u|^2 summed by component. */
+static double pos_q_md(int nv, int which, const double *W)
+{
+    if (which == 0) return W[0];
+    double rho = W[0], q2 = 0.0;
+    for (int i = 1; i < nv - 1; i++) {
+        double u = W[i] / rho;
+        q2 = q2 + u * u;
+    }
+    double ekin = 0.5 * q2;
+    double p = (G - 1) * (W[nv - 1] - rho * ekin);
+    return G * p;
+}
+
+static void pos_limit_md(int nv, int which, const double *W, double *Wi)
+{
+    double qi = pos_q_md(nv, which, Wi);
+    if (qi >= 1e-10) return;
+    double q = pos_q_md(nv, which, W);
+    if (q < 1e-10) { for (int i = 0; i < nv; i++) Wi[i] = W[i]; return; }
+    double th = (1e-10 - q) / (qi - q);
+    for (int i = 0; i < nv; i++) Wi[i] = (1 - th) * W[i] + th * Wi[i];
+}
+
 /* reconI for the face between stencil cells 2 and 3 */
 static void recon_face(const orc_cfg *c, int ax, double (*P)[MAXV], double *fl, double *fr)
 {
@@ -295,6 +321,18 @@ static void recon_face(const orc_cfg *c, int ax, double (*P)[MAXV], double *fl, 
         pos_limit(1, WL, cl); pos_limit(1, WR, cr);
         back_to_prim(3, cl, fl);
         back_to_prim(3, cr, fr);
+        return;
+    }
+    if (c->posl) {
+        /* the 1D limiter (positive_preserving.hpp:13-46, reconstructor5order.hpp:225-236)
+           on the 2D/3D cons: rho of both states, then gamma p of both */
+        double WL[MAXV], WR[MAXV];
+        p2c(nv, P[2], WL);
+        p2c(nv, P[3], WR);
+        pos_limit_md(nv, 0, WL, cl); pos_limit_md(nv, 0, WR, cr);
+        pos_limit_md(nv, 1, WL, cl); pos_limit_md(nv, 1, WR, cr);
+        back_to_prim(nv, cl, fl);
+        back_to_prim(nv, cr, fr);
         return;
     }
     back_to_prim(nv, cl, fl);

@@ -32,6 +32,8 @@ typedef struct orc_cfg {
                          ORC_MIRRORCOPY (PERIODIC1D with the reference's default wiring) */
     int threads;      /* OpenMP threads (0 = runtime default) */
     int diff;         /* 0: MND6 (4 ghosts), 1: TRAD6 (ExplicitDif6, 5 ghosts) */
+    int posl;         /* 2D/3D: 1 = the 1D positivity limiter on the face states (the library's
+                         cfd_config.positivity) instead of the reference's cell-state fallback */
 } orc_cfg;
 
 /* rhs (AoS, ncell*nvar) of cons (AoS) */

@@ -219,7 +219,8 @@ ORC_FAMILY = {2: (0, 0.0), 3: (1, 0.0), 11: (2, 1e-5), 12: (2, 1e-4), 13: (2, 1e
 
 class OrcCfg(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("h", C.c_double), ("fam", C.c_int), ("icst", C.c_double),
-                ("flux", C.c_int), ("bc", (C.c_int * 2) * 3), ("threads", C.c_int), ("diff", C.c_int)]
+                ("flux", C.c_int), ("bc", (C.c_int * 2) * 3), ("threads", C.c_int), ("diff", C.c_int),
+                ("posl", C.c_int)]
 
 
 _orc = None
@@ -247,13 +248,14 @@ def orc_load() -> C.CDLL:
 class OracleC:
     """The plain-C restatement (1D/2D/3D) on a uniform grid with per-side BC kinds."""
 
-    def __init__(self, dim, n, h, inter_method=2, flux_method=0, bc=None, threads=0, trad6=False):
+    def __init__(self, dim, n, h, inter_method=2, flux_method=0, bc=None, threads=0, trad6=False, positivity=False):
         self.lib = orc_load()
         fam, icst = ORC_FAMILY[inter_method]
         n3 = list(n) + [1] * (3 - len(n))
         bcs = bc if bc is not None else [[ORC_OUTLET] * 2] * 3
         arr = ((C.c_int * 2) * 3)(*[(C.c_int * 2)(*bcs[d]) for d in range(3)])
-        self.cfg = OrcCfg(dim, (C.c_int * 3)(*n3), h, fam, icst, flux_method, arr, threads, int(bool(trad6)))
+        self.cfg = OrcCfg(dim, (C.c_int * 3)(*n3), h, fam, icst, flux_method, arr, threads, int(bool(trad6)),
+                          int(bool(positivity)))
         self.nvar = dim + 2
         self.ncell = n3[0] * n3[1] * n3[2]
         self.cons = None

@@ -285,3 +285,39 @@ def test_adjoint_rejects_unsupported_configurations():
     with pytest.raises(_lib.CfdError) as e:
         p.adjoint_reverse(np.zeros((256, 4)))
     assert e.value.code == -1
+
+
+def test_adjoint_full_configuration_against_reference_solver_fd(ref):
+    """The adjoint configuration (256^2 periodic, WCNS5 + Roe, 400 frozen-dt
+    RK3 steps, checkpoints every 20, J = sum of rho^2 over 64 seeded probes)
+    against finite differences of the reference solver's own RK3_SSP steps
+    (zone_FD compiled from its sources), along 3 seeded directions of the
+    initial density at fixed velocity and pressure (Richardson central
+    differences, density step 1e-6), to 1e-6 relative."""
+    from cfd_inwsl_b200.cases import adjoint_problem
+    n, nsteps = 256, 400
+    U0, probes = adjoint_problem(n, seed=0)
+    info = make_info(2, [n, n], [0, 1, 0, 1, 0, 0], im=2, fm=1)
+    s = zone.BlockSolver(info, periodic=True)
+    s.set_cons(U0)
+    dt = s.getTimeIntervalExplicit()
+    s.adjoint_record(dt, nsteps, 20)
+    g = s.adjoint_reverse(seed(s.cons, probes))
+    s.close()
+    r = ref.RefSolver(2, [n, n], [0, 1, 0, 1, 0, 0], inter_method=2, flux_method=1, n_case=0, periodic=True)
+
+    def ref_J(U):
+        r.cons = U
+        for _ in range(nsteps):
+            r.solve(dt)
+        return objective(r.cons, probes)
+
+    rng = np.random.default_rng(33)
+    u, v = U0[:, 1] / U0[:, 0], U0[:, 2] / U0[:, 0]
+    for _ in range(3):
+        dr = rng.normal(size=n * n)
+        d = np.stack([dr, u * dr, v * dr, 0.5 * (u * u + v * v) * dr], -1)
+        fd = richardson(lambda e: ref_J(U0 + e * d), eps=1e-6)
+        ad = float(np.sum(g * d))
+        assert abs(fd - ad) <= TOL * max(abs(fd), abs(ad)), (fd, ad)
+    r.close()

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from cfd_inwsl_b200 import _lib, zone
-from tests.util import gpu_solver, quadrant_state, rel_linf, smooth_state_3d
+from tests.util import gpu_solver, make_info, quadrant_state, rel_linf, smooth_state_3d
 
 pytestmark = pytest.mark.gpu
 GOLD = Path(__file__).resolve().parent / "golden"
@@ -367,3 +367,69 @@ def test_mixed_face_close_to_fp64_face():
             fmx = _lib.eval_face(2, ax, im, P, precision=1)
             scale = np.abs(P[:, 2:4] - P[:, 2:3]).max() + 1e-30
             assert np.abs(fmx - f64).max() < 1e-5 * max(scale, 1.0), (im, ax, np.abs(fmx - f64).max())
+
+
+def test_shared_reciprocal_division_is_ieee_division():
+    """The strict flavour divides by shared correctly rounded reciprocals
+    (Markstein's correction). On the device it must give IEEE division's bits
+    on every operand class: random, next to rounding midpoints, physical
+    ranges, signed zeros, tiny and huge dividends."""
+    import ctypes as C
+    bad = C.c_ulonglong(99)
+    for seed in (1, 2, 3):
+        _lib.check(_lib.load().cfd_check_division(1 << 26, seed, C.byref(bad)))
+        assert bad.value == 0, (seed, bad.value)
+
+
+# ----------------------------------------------------------------- the positivity option (2D/3D)
+def near_vacuum_2d(n, rng):
+    """A near-vacuum bubble (rho = 1e-3, p = 1e-4 within radius 0.2) in a
+    still gas at rest: fifth-order face states at its edge undershoot to
+    rho or p < 0, where the positivity option acts."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x)
+    inside = (X - 0.5) ** 2 + (Y - 0.5) ** 2 < 0.04
+    rho = np.where(inside, 1e-3, 1.0) * (1 + 0.01 * rng.uniform(size=X.shape))
+    p = np.where(inside, 1e-4, 1.0)
+    return zone.prim_to_cons(np.stack([rho, 0 * X, 0 * X, p], -1).reshape(-1, 4))
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_positivity_option_against_oracle(strict):
+    """cfd_config.positivity = 1 applies the reference's 1D limiter to the 2D
+    face states; RHS and RK3 steps against the C restatement with the same
+    option (bit for bit in the strict flavour), on a state where the limiter
+    acts (the option changes the RHS) and on a smooth one (it does not)."""
+    from oracle.refsolver import ORC_OUTLET, OracleC
+    rng = np.random.default_rng(123)
+    n = 48
+    for state, acts in ((near_vacuum_2d(n, rng), True), (smooth_state_2d(n, rng), False)):
+        info = make_info(2, [n, n], im=2, fm=0, strict=strict)
+        info.positivity = 1
+        s = zone.BlockSolver(info)
+        s0 = gpu_solver(2, [n, n], im=2, fm=0, strict=strict)
+        o = OracleC(2, [n, n], 1.0 / n, 2, 0, bc=[[ORC_OUTLET] * 2] * 3, positivity=True)
+        s.set_cons(state)
+        s0.set_cons(state)
+        o.cons = state
+        rg, ro, r0 = s.rhsSolve(), o.rhs(), s0.rhsSolve()
+        assert (not np.array_equal(rg, r0)) == acts
+        dt = o.max_dt(0.3)
+        s.solve(dt)
+        o.solve(dt)
+        if strict:
+            np.testing.assert_array_equal(rg, ro)
+            np.testing.assert_array_equal(s.cons, o.cons)
+        else:
+            assert rel_linf(rg, ro) < 1e-10 and rel_linf(s.cons, o.cons) < 1e-12
+        assert np.all(s.cons[:, 0] > 0)
+        for x in (s, s0):
+            x.close()
+
+
+def smooth_state_2d(n, rng):
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x)
+    rho = 1 + 0.2 * np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y)
+    prim = np.stack([rho, 0.3 + 0 * X, -0.2 + 0 * X, 1 + 0.1 * np.cos(2 * np.pi * (X + Y))], -1).reshape(-1, 4)
+    return zone.prim_to_cons(prim)

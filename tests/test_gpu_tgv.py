@@ -68,3 +68,37 @@ def test_tgv_mixed_energy_history_close_to_fp64():
     dev = np.max(np.abs(k32 - k64) / k64)
     print("max relative KE deviation, mixed vs FP64:", dev)
     assert dev < 1e-9
+
+
+def test_tgv_64_energy_history_100_steps():
+    """The throughput configuration's physics at 64^3: 100 CFL steps (CFL 0.5,
+    WCNS5 + HLLC). The strict flavour's dt, state and kinetic-energy history
+    equal the C restatement's bit for bit at every step; the fast flavour,
+    taking its own dt, stays within 1e-10 relative L-inf of the strict state
+    after the 100 steps (the WCNS5 weights are continuous: FMA rounding cannot
+    switch a stencil)."""
+    from oracle.refsolver import ORC_WRAP, OracleC
+    from tests.util import rel_linf
+    n, steps = 64, 100
+    c, h = cases.tgv_state(n)
+    zone_ = [0, 2 * np.pi, 0, 2 * np.pi, 0, 2 * np.pi]
+    s = gpu_solver(3, [n] * 3, zone_, im=2, fm=0, strict=True, periodic=True)
+    f = gpu_solver(3, [n] * 3, zone_, im=2, fm=0, strict=False, periodic=True)
+    o = OracleC(3, [n] * 3, s.info.geth(0), 2, 0, bc=[[ORC_WRAP] * 2] * 3)
+    s.set_cons(c)
+    f.set_cons(c)
+    o.cons = c
+    ke_o, ke_g = [cases.kinetic_energy(c, h)], [cases.kinetic_energy(c, h)]
+    for _ in range(steps):
+        dt = o.max_dt(0.5)
+        assert s.getTimeIntervalExplicit() == dt
+        o.solve(dt)
+        s.solve(dt)
+        f.solve(f.getTimeIntervalExplicit())
+        ke_o.append(cases.kinetic_energy(o.cons, h))
+        ke_g.append(cases.kinetic_energy(s.cons, h))
+    np.testing.assert_array_equal(s.cons, o.cons)
+    assert ke_g == ke_o
+    assert rel_linf(f.cons, s.cons) <= 1e-10
+    for x in (s, f):
+        x.close()
