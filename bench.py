@@ -710,7 +710,7 @@ def run_ours(args, rank, world, local_rank):
         adjoint = adjoint_cost(local_rank, stream, nsteps=args.adjoint_steps)
     batch = None
     if not args.no_batch and world == 1:
-        batch = batch_throughput(local_rank, stream, full_run=not args.no_batch_full)
+        batch = batch_throughput(local_rank, stream, full_run=args.batch_full)
     tgv = None
     if not args.no_tgv and world == 1 and dim == 2:
         tgv = tgv_block(local_rank, stream, peak_tflops=peak_tflops)
@@ -774,7 +774,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--no-batch-full", action="store_true", help="skip the batched run to t = 0.25")
+    ap.add_argument("--batch-full", action="store_true",
+                    help="also run the whole batched configuration to t = 0.25 (about 2.5 minutes)")
     ap.add_argument("--no-tgv", action="store_true", help="skip the 3D Taylor-Green block")
     ap.add_argument("--force-slabs", action="store_true",
                     help="run the multi-GPU slab path (halo exchange) even on one GPU (one periodic slab)")

@@ -382,7 +382,13 @@ struct cfd_handle {
     // and one full segment's recomputation and reverse sweep; valid for
     // (adj_graph_K, adj_graph_dt)
     cudaGraphExec_t adj_rec_graph[3] = {nullptr, nullptr, nullptr};
-    cudaGraphExec_t adj_rev_graph = nullptr;
+    // the reverse pass, per stage-buffer set: the segment's recomputation (on
+    // adj_aux) and its reverse sweep (on the handle's stream)
+    cudaGraphExec_t adj_recomp_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t adj_back_graph[2] = {nullptr, nullptr};
+    std::vector<double *> adj_stage_b;   // the second set of stage states (overlap)
+    cudaStream_t adj_aux = nullptr;      // recomputation stream of the reverse pass
+    cudaEvent_t adj_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // recomputed[set], reversed[set]
     int adj_graph_K = 0;
     double adj_graph_dt = 0.0;
     // slab decomposition: halo rows of the last direction's low / high side
@@ -633,8 +639,11 @@ void drop_graphs(cfd_handle *h)
         if (h->adj_rec_graph[k]) cudaGraphExecDestroy(h->adj_rec_graph[k]);
         h->adj_rec_graph[k] = nullptr;
     }
-    if (h->adj_rev_graph) cudaGraphExecDestroy(h->adj_rev_graph);
-    h->adj_rev_graph = nullptr;
+    for (int k = 0; k < 2; k++) {
+        if (h->adj_recomp_graph[k]) cudaGraphExecDestroy(h->adj_recomp_graph[k]);
+        if (h->adj_back_graph[k]) cudaGraphExecDestroy(h->adj_back_graph[k]);
+        h->adj_recomp_graph[k] = h->adj_back_graph[k] = nullptr;
+    }
     h->adj_graph_K = 0;
 }
 
@@ -869,7 +878,14 @@ void cfd_destroy(cfd_handle *h)
     for (double *b : h->adj_buf) cudaFree(b);
     cudaFree(h->halo[0]);
     cudaFree(h->halo[1]);
+    for (double *b : h->adj_stage_b) cudaFree(b);
     drop_graphs(h);
+    if (h->adj_aux) {
+        cudaStreamSynchronize(h->adj_aux);
+        cudaStreamDestroy(h->adj_aux);
+    }
+    for (cudaEvent_t ev : h->adj_ev)
+        if (ev) cudaEventDestroy(ev);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
@@ -2021,23 +2037,36 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
     CFD_CUDA(h, cudaMemcpyAsync(h->stage, dJ_dUN_aos, state, cudaMemcpyHostToDevice, h->stream));
     if ((rc = launch_aos_to_soa(h, h->stage, lam))) return rc;
     const int nseg = (N + K - 1) / K;
-    // one segment of cnt steps whose first state is in adj_stage[0]
-    auto segment = [&](int cnt) -> int {
+    // Two sets of stage states: while the reverse sweep of segment s runs on
+    // the handle's stream from one set, segment s - 1 is recomputed from its
+    // checkpoint into the other on a second stream; events order each set's
+    // reuse. Both passes are latency bound on the adjoint's grids, so they
+    // share the SMs instead of running one after the other.
+    if ((rc = adjoint_states(h, h->adj_stage_b, 3 * (size_t)K + 1))) return rc;
+    if (!h->adj_aux) CFD_CUDA(h, cudaStreamCreateWithFlags(&h->adj_aux, cudaStreamNonBlocking));
+    for (int k = 0; k < 4; k++)
+        if (!h->adj_ev[k]) CFD_CUDA(h, cudaEventCreateWithFlags(&h->adj_ev[k], cudaEventDisableTiming));
+    std::vector<double *> *sets[2] = {&h->adj_stage, &h->adj_stage_b};
+    // recompute cnt steps from st[0], keeping every stage state
+    auto recompute = [&](std::vector<double *> &st, int cnt) -> int {
         int r;
-        // recompute the segment, keeping every stage state
         for (int j = 0; j < cnt; j++) {
-            double *S[3] = {h->adj_stage[3 * j], h->adj_stage[3 * j + 1], h->adj_stage[3 * j + 2]};
-            if (j + 1 < cnt && (r = adjoint_step(h, dt, S, h->adj_stage[3 * (j + 1)]))) return r;
+            double *S[3] = {st[3 * j], st[3 * j + 1], st[3 * j + 2]};
+            if (j + 1 < cnt && (r = adjoint_step(h, dt, S, st[3 * (j + 1)]))) return r;
             if (j + 1 == cnt) {
                 // the last step's stages only (its output is not needed)
                 if ((r = rk_stage(h, 1, S[0], S[0], S[1], 1.0, dt, 0.0, 0.0, false))) return r;
                 if ((r = rk_stage(h, 2, S[1], S[0], S[2], 0.75, 0.25 * dt, 0.25, 0.0, false))) return r;
             }
         }
-        // reverse through the segment's steps:
-        //   U1 = U0 - dt R(U0); U2 = 3/4 U0 + 1/4 (U1 - dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 - dt R(U2))
+        return CFD_OK;
+    };
+    // reverse through the segment's steps:
+    //   U1 = U0 - dt R(U0); U2 = 3/4 U0 + 1/4 (U1 - dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 - dt R(U2))
+    auto back = [&](std::vector<double *> &st, int cnt) -> int {
+        int r;
         for (int j = cnt - 1; j >= 0; j--) {
-            double *U0 = h->adj_stage[3 * j], *U1 = h->adj_stage[3 * j + 1], *U2 = h->adj_stage[3 * j + 2];
+            double *U0 = st[3 * j], *U1 = st[3 * j + 1], *U2 = st[3 * j + 2];
             // lam2 = 2/3 (lam3 - dt J(U2)^T lam3)
             if ((r = rhs_vjp(h, U2, lam, vjp_out(w, lam, 2.0 / 3.0, -2.0 / 3.0 * dt)))) return r;
             // lam1 = 1/4 (lam2 - dt J(U1)^T lam2); lam = lam3 / 3 + 3/4 lam2
@@ -2054,17 +2083,57 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
         h->adj_graph_K = K;
         h->adj_graph_dt = dt;
     }
-    for (int seg = nseg - 1; seg >= 0; seg--) {
-        const int s0 = seg * K, cnt = std::min(K, N - s0);
-        CFD_CUDA(h, cudaMemcpyAsync(h->adj_stage[0], h->adj_ckpt[seg], state, cudaMemcpyDeviceToDevice, h->stream));
-        if (cnt == K) {  // full segments replay one captured graph
-            if (!h->adj_rev_graph && (rc = capture_graph(h, [&] { return segment(K); }, &h->adj_rev_graph)))
-                return rc;
-            CFD_CUDA(h, cudaGraphLaunch(h->adj_rev_graph, h->stream));
-            h->launches += (3ULL * h->dim + 9ULL) * K;
-        } else if ((rc = segment(cnt))) {
-            return rc;
+    cudaStream_t main_st = h->stream, aux = h->adj_aux;
+    // the recomputation stream starts after everything queued so far
+    CFD_CUDA(h, cudaEventRecord(h->adj_ev[2], main_st));
+    CFD_CUDA(h, cudaStreamWaitEvent(aux, h->adj_ev[2], 0));
+    auto launch_recompute = [&](int seg, int set) -> int {
+        const int cnt = std::min(K, N - seg * K);
+        std::vector<double *> &st = *sets[set];
+        h->stream = aux;  // every launch of the recomputation goes to the second stream
+        int r = CFD_OK;
+        cudaError_t e = cudaMemcpyAsync(st[0], h->adj_ckpt[seg], state, cudaMemcpyDeviceToDevice, aux);
+        if (e != cudaSuccess) r = cuda_fail(h, e, "checkpoint copy");
+        if (!r && cnt == K) {
+            if (!h->adj_recomp_graph[set])
+                r = capture_graph(h, [&] { return recompute(st, K); }, &h->adj_recomp_graph[set]);
+            if (!r && (e = cudaGraphLaunch(h->adj_recomp_graph[set], aux)) != cudaSuccess) r = cuda_fail(h, e, "graph");
+            if (!r) h->launches += 3ULL * h->dim * K;
+        } else if (!r) {
+            r = recompute(st, cnt);
         }
+        h->stream = main_st;
+        if (!r && (e = cudaEventRecord(h->adj_ev[set], aux)) != cudaSuccess) r = cuda_fail(h, e, "event");
+        return r;
+    };
+    auto launch_back = [&](int seg, int set) -> int {
+        const int cnt = std::min(K, N - seg * K);
+        std::vector<double *> &st = *sets[set];
+        cudaError_t e = cudaStreamWaitEvent(main_st, h->adj_ev[set], 0);
+        if (e != cudaSuccess) return cuda_fail(h, e, "event wait");
+        int r;
+        if (cnt == K) {
+            if (!h->adj_back_graph[set] && (r = capture_graph(h, [&] { return back(st, K); }, &h->adj_back_graph[set])))
+                return r;
+            if ((e = cudaGraphLaunch(h->adj_back_graph[set], main_st)) != cudaSuccess) return cuda_fail(h, e, "graph");
+            h->launches += 9ULL * K;
+        } else if ((r = back(st, cnt))) {
+            return r;
+        }
+        if ((e = cudaEventRecord(h->adj_ev[2 + set], main_st)) != cudaSuccess) return cuda_fail(h, e, "event");
+        return CFD_OK;
+    };
+    bool used[2] = {false, false};
+    if ((rc = launch_recompute(nseg - 1, 0))) return rc;
+    for (int seg = nseg - 1; seg >= 0; seg--) {
+        const int set = (nseg - 1 - seg) & 1, other = set ^ 1;
+        if (seg > 0) {
+            // the other set is free once the reverse sweep that read it is done
+            if (used[other]) CFD_CUDA(h, cudaStreamWaitEvent(aux, h->adj_ev[2 + other], 0));
+            if ((rc = launch_recompute(seg - 1, other))) return rc;
+        }
+        if ((rc = launch_back(seg, set))) return rc;
+        used[set] = true;
     }
     if ((rc = launch_soa_to_aos(h, lam, h->stage, 0))) return rc;
     CFD_CUDA(h, cudaMemcpyAsync(dJ_dU0_aos, h->stage, state, cudaMemcpyDeviceToHost, h->stream));
