@@ -33,53 +33,42 @@
 namespace cfd {
 namespace CFD_NS {
 
-// Ghost cell k (0 = nearest the boundary) of a line end, as OneDBnd::update
-// leaves it after Bnds::update (oneDBnd.cpp:31-114). The copying types only
-// name the cell (or halo row) whose cons the ghost takes, so that the sweep
-// loads and converts every cell, interior or ghost, through one code path:
-// ghost_source returns the cons' address and the stride between their
-// variables, and the velocity component a mirror negates; static and analytic
-// ghosts (DIRICLET and every type whose update() is a no-op, DoubleMachUp)
-// give their prim directly (ghost_static_prim).
-struct GhostSrc {
-    const double *cons;  // null: static or analytic prim (ghost_static_prim)
-    long long stride;    // between the cons' variables
-    int neg;             // velocity component to negate (1..NV-2), 0: none
-};
-
 template <int NV>
-__device__ __forceinline__ GhostSrc ghost_source(const SweepParams &p, const BcLine &bl, int k)
+__device__ __forceinline__ void load_cons_prim(const double *__restrict__ u, long long ncell, long long cell,
+                                               double *pr)
+{
+    double c[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) c[v] = __ldg(u + v * ncell + cell);
+    cons_to_prim<NV>(c, pr);
+}
+
+// Ghost cell k (0 = nearest the boundary) of a line end, as OneDBnd::update
+// leaves it after Bnds::update (oneDBnd.cpp:31-114).
+template <int NV, int NG>
+__device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &bl, int k, double tstage, double *pr)
 {
     switch (bl.type) {
     case BND_PERIODIC1D:
-        return GhostSrc{p.u + bl.i0 + (long long)k * bl.offset, p.ncell, 0};
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0 + (long long)k * bl.offset, pr);
+        return;
     case BND_SUPERSONICOUTLET:
-        return GhostSrc{p.u + bl.i0, p.ncell, 0};
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0, pr);
+        return;
     case BND_SYMMETRYX:
     case BND_SYMMETRYY:
     case BND_SYMMETRYZ:
     case BND_SYMMETRY1D: {
-        const int neg = (bl.type == BND_SYMMETRYY) ? 2 : (bl.type == BND_SYMMETRYZ) ? 3 : 1;
-        return GhostSrc{p.u + bl.i0 + (long long)k * bl.offset, p.ncell, neg < NV - 1 ? neg : 0};
+        load_cons_prim<NV>(p.u, p.ncell, bl.i0 + (long long)k * bl.offset, pr);
+        int neg = (bl.type == BND_SYMMETRYY) ? 2 : (bl.type == BND_SYMMETRYZ) ? 3 : 1;
+        if (neg < NV - 1) pr[neg] = -pr[neg];
+        if (bl.type == BND_SYMMETRY1D) {
+            // SYMMETRY1D writes only the first three values of each ghost cell.
+            for (int v = 3; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * NG + k) * NV + v] : 0.0;
+        }
+        return;
     }
-    case BND_HALO: {
-        // rows of the neighbouring slab, ascending: the low side's nearest
-        // ghost is the neighbour's last row, the high side's its first
-        const int kk = k > 3 ? 3 : k;  // four halo rows (MND6 only)
-        const int r = (bl.offset == 0) ? 3 - kk : kk;
-        const double *hb = (bl.offset == 0) ? p.halo_lo : p.halo_hi;
-        return GhostSrc{hb + (long long)r * p.halo_nl + bl.i0, 4 * p.halo_nl, 0};
-    }
-    default:
-        return GhostSrc{nullptr, 0, 0};
-    }
-}
-
-template <int NV, int NG>
-__device__ __forceinline__ void ghost_static_prim(const SweepParams &p, const BcLine &bl, int k, double tstage,
-                                                  double *pr)
-{
-    if (bl.type == BND_DOUBLEMACHUP) {
+    case BND_DOUBLEMACHUP: {
         // oneDBnd.cpp:87-108: exact post- or pre-shock state at the stage time.
         // As in the reference, ghost k is placed at y = -dh/2 + k*dh (measured
         // from 0, not from the line end) and x is the edge cell's centre.
@@ -94,8 +83,23 @@ __device__ __forceinline__ void ghost_static_prim(const SweepParams &p, const Bc
         if (NV == 5) pr[3] = 0.0;
         return;
     }
-    // DIRICLET and every type whose update() is a no-op keep their static data.
-    for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * NG + k) * NV + v] : 0.0;
+    case BND_HALO: {
+        // rows of the neighbouring slab, ascending: the low side's nearest
+        // ghost is the neighbour's last row, the high side's its first
+        const int kk = k > 3 ? 3 : k;  // four halo rows (MND6 only)
+        const int r = (bl.offset == 0) ? 3 - kk : kk;
+        const double *hb = (bl.offset == 0) ? p.halo_lo : p.halo_hi;
+        double c[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) c[v] = hb[((long long)v * 4 + r) * p.halo_nl + bl.i0];
+        cons_to_prim<NV>(c, pr);
+        return;
+    }
+    default:
+        // DIRICLET and every type whose update() is a no-op keep their static data.
+        for (int v = 0; v < NV; v++) pr[v] = (bl.slot >= 0) ? p.bc_vals[((long long)bl.slot * NG + k) * NV + v] : 0.0;
+        return;
+    }
 }
 
 #ifndef CFD_SWEEP_MINB
@@ -236,53 +240,33 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 
     // Stage cell P (global index along AX, may be a ghost) of line l; staged:
     // its cons already sit in stg[0] (interior cells of the thread's own line).
-    auto load_pos = [&](int l, int P, bool staged) {
+    auto load_pos = [&](int l, int P, bool staged = false) {
         bool ok; long long base; int lid;
         if (PREC == 1 && l == tl) own_line(ok, base, lid);
         else line_of(l, ok, base, lid);
         double pr[NV];
         double cs[NV];
         bool have_cs = false;  // the mixed form takes interior cells' cons as loaded
-        // the cell's cons: staged, from the grid or a halo row (src), or none
-        // (a static or analytic ghost, or a line past the grid's edge)
-        const double *src = nullptr;
-        long long sstride = p.ncell;
-        int neg = 0;
-        const BcLine *bl = nullptr;
-        int k = 0;
-        const bool interior = P >= 0 && P < nd;
         if (!ok) {
             pr[0] = 1.0;
             for (int v = 1; v < NV - 1; v++) pr[v] = 0.0;
             pr[NV - 1] = 1.0;
-        } else if (interior) {
-            src = p.u + base + (long long)P * sAX;
-        } else {
-            k = (P < 0) ? -P - 1 : P - nd;
-            k = k > HG - 1 ? HG - 1 : k;
-            bl = (P < 0) ? p.bc_lo + lid : p.bc_hi + lid;
-            const GhostSrc g = ghost_source<NV>(p, *bl, k);
-            src = g.cons;
-            sstride = g.stride;
-            neg = g.neg;
-            if (!src) ghost_static_prim<NV, HG>(p, *bl, k, tstage, pr);
-        }
-        if (ok && src) {
-            if (interior && staged) {
+        } else if (P >= 0 && P < nd) {
+            if (staged) {
 #pragma unroll
                 for (int v = 0; v < NV; v++) cs[v] = stg[v * NT + threadIdx.x];
             } else {
 #pragma unroll
-                for (int v = 0; v < NV; v++) cs[v] = __ldg(src + v * sstride);
+                for (int v = 0; v < NV; v++) cs[v] = __ldg(p.u + v * p.ncell + base + (long long)P * sAX);
             }
             cons_to_prim<NV>(cs, pr);
-            if (neg) pr[neg] = -pr[neg];
-            if (bl && bl->type == BND_SYMMETRY1D) {
-                // SYMMETRY1D writes only the first three values of each ghost cell
-                for (int v = 3; v < NV; v++)
-                    pr[v] = (bl->slot >= 0) ? p.bc_vals[((long long)bl->slot * HG + k) * NV + v] : 0.0;
-            }
-            have_cs = (PREC == 1) && interior;
+            have_cs = (PREC == 1);
+        } else if (P < 0) {
+            int k = -P - 1;
+            ghost_prim<NV, HG>(p, p.bc_lo[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
+        } else {
+            int k = P - nd;
+            ghost_prim<NV, HG>(p, p.bc_hi[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
         }
         if (!have_cs) prim_to_cons<NV>(pr, cs);  // as the reference's primToChar re-derives them
         int slot = ring(P - s_begin + HG);
@@ -361,6 +345,13 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
         for (int v = 0; v < NV; v++) sf[(v * W + l) * LSF + fslot] = fx[v];
     };
 
+    // prologue: cells s_begin-HG .. s_begin+HG-1
+    for (int idx = tid; idx < 2 * HG * W; idx += NT) {
+        int l = (AX == 0) ? idx / (2 * HG) : idx % W;
+        int q = (AX == 0) ? idx % (2 * HG) : idx / W;
+        load_pos(l, s_begin - HG + q);
+    }
+
     double red_rho = 0.0, red_lam[3] = {0.0, 0.0, 0.0};
     unsigned err = 0;
 
@@ -396,27 +387,13 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     if constexpr (PF) prefetch_cell(s_begin + HG + tp);
 
     for (int c0 = s_begin; c0 < s_end; c0 += S) {
-        if constexpr (PF) __pipeline_wait_prior(0);
-        {
-            // the chunk's S new cells per line, and before the segment's first
-            // chunk also its 2 HG cells s_begin-HG .. s_begin+HG-1, from one
-            // call site (the load and conversion code is emitted once)
-            const int nload = (c0 == s_begin) ? NT + 2 * HG * W : NT;
-#pragma unroll 1
-            for (int idx = tid; idx < nload; idx += NT) {
-                if (idx < NT) {
-                    load_pos(tl, c0 + HG + tp, PF);
-                } else {
-                    const int e = idx - NT;
-                    const int l = (AX == 0) ? e / (2 * HG) : e % W;
-                    const int q = (AX == 0) ? e % (2 * HG) : e / W;
-                    load_pos(l, s_begin - HG + q, false);
-                }
-            }
-        }
         if constexpr (PF) {
+            __pipeline_wait_prior(0);
+            load_pos(tl, c0 + HG + tp, true);
             prefetch_epilogue(c0 + tp);
             prefetch_cell(c0 + S + HG + tp);  // an empty group past the segment
+        } else {
+            load_pos(tl, c0 + HG + tp);
         }
         __syncthreads();
         {
@@ -424,7 +401,6 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             // chunk also the FC faces ahead of them, from one call site (the
             // face code is emitted once)
             const int nface = (c0 == s_begin) ? NT + FC * W : NT;
-#pragma unroll 1
             for (int idx = tid; idx < nface; idx += NT) {
                 int l, j;
                 if (idx < NT) {
