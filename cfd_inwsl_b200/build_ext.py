@@ -52,7 +52,7 @@ def units() -> list[tuple[Path, Path, list[str]]]:
     out.append((CSRC / "api.cu", BUILD / "api.o", ["--fmad=false", "-DCFD_NS=api"],
                 headers + [CSRC / "sweep_dispatch.h", CSRC / "adjoint.h", ROOT / "include" / "cfdgpu.h"]))
     out.append((CSRC / "adjoint.cu", BUILD / "adjoint.o", ["--fmad=true", "-DCFD_FAST", "-DCFD_NS=adj"],
-                [CSRC / "euler_math.cuh", CSRC / "adjoint.h"]))
+                [CSRC / "euler_math.cuh", CSRC / "adjoint.h", CSRC / "adjoint_math.h"]))
     out.append((CSRC / "noalloc.cu", BUILD / "noalloc.o", ["--fmad=false", "-DCFD_NS=api"],
                 headers + [CSRC / "sweep_dispatch.h", ROOT / "include" / "cfdgpu.h"]))
     return out

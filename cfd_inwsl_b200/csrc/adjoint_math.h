@@ -35,25 +35,43 @@ constexpr double kGG1 = kGam / (kGam - 1.0);
 constexpr double kW0 = 3.0 / 2.0, kW1 = -3.0 / 10.0, kW2 = 1.0 / 30.0;
 constexpr int kCharsUnroll = ADJ_CHARS_UNROLL;
 
-// cons (rho, rho u, rho v, rho E) -> prim (rho, u, v, p)
-ADJ_HD void c2p(const double *c, double *p)
+// cons (rho, rho u, rho v, rho E) -> prim (rho, u, v, p); returns 1/rho
+ADJ_HD double c2p(const double *c, double *p)
 {
     const double ir = 1.0 / c[0];
     p[0] = c[0];
     p[1] = c[1] * ir;
     p[2] = c[2] * ir;
     p[3] = kGm1 * (c[3] - (c[1] * c[1] + c[2] * c[2]) * (0.5 * ir));
+    return ir;
 }
 
-// cb += (d prim / d cons)^T pb, p = c2p(c)
-ADJ_HD void c2p_adj(const double *c, const double *p, const double *pb, double *cb)
+// cb += (d prim / d cons)^T pb, p = c2p(c), ir = 1/rho as c2p returned it
+ADJ_HD void c2p_adj(const double *p, double ir, const double *pb, double *cb)
 {
-    const double ir = 1.0 / c[0];
     const double u = p[1], v = p[2];
     cb[0] += pb[0] - (u * pb[1] + v * pb[2]) * ir + pb[3] * (0.5 * kGm1) * (u * u + v * v);
     cb[1] += pb[1] * ir - pb[3] * kGm1 * u;
     cb[2] += pb[2] * ir - pb[3] * kGm1 * v;
     cb[3] += pb[3] * kGm1;
+}
+
+// 1/s0, 1/s1, 1/s2 from one division of their product (three divisions
+// cost about three times as much on the FP64 pipe); the product is guarded
+// against overflow (s_k >= 1e-6 here, so it cannot underflow)
+ADJ_HD void recip3(double s0, double s1, double s2, double &r0, double &r1, double &r2)
+{
+    const double s01 = s0 * s1, p = s01 * s2;
+    if (p < 1e300) {
+        const double ip = 1.0 / p;
+        r0 = (s1 * s2) * ip;
+        r1 = (s0 * s2) * ip;
+        r2 = s01 * ip;
+    } else {
+        r0 = 1.0 / s0;
+        r1 = 1.0 / s1;
+        r2 = 1.0 / s2;
+    }
 }
 
 // weno5_JSchen: gamma_k / (1e-6 + beta_k)^2 weights of the three candidates
@@ -64,7 +82,9 @@ ADJ_HD double wcns5(const double *q)
     const double a2 = q[2] - 2.0 * q[3] + q[4], b2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
     const double s0 = 1e-6 + a0 * a0 + 0.25 * b0 * b0, s1 = 1e-6 + a1 * a1 + 0.25 * b1 * b1,
                  s2 = 1e-6 + a2 * a2 + 0.25 * b2 * b2;
-    const double al0 = (1.0 / 16.0) / (s0 * s0), al1 = (5.0 / 8.0) / (s1 * s1), al2 = (5.0 / 16.0) / (s2 * s2);
+    double r0, r1, r2;
+    recip3(s0, s1, s2, r0, r1, r2);
+    const double al0 = (1.0 / 16.0) * (r0 * r0), al1 = (5.0 / 8.0) * (r1 * r1), al2 = (5.0 / 16.0) * (r2 * r2);
     const double u0 = 0.375 * q[0] - 1.25 * q[1] + 1.875 * q[2];
     const double u1 = -0.125 * q[1] + 0.75 * q[2] + 0.375 * q[3];
     const double u2 = 0.375 * q[2] + 0.75 * q[3] - 0.125 * q[4];
@@ -79,7 +99,9 @@ ADJ_HD void wcns5_adj(const double *q, double Qb, double *qb)
     const double a2 = q[2] - 2.0 * q[3] + q[4], b2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
     const double s0 = 1e-6 + a0 * a0 + 0.25 * b0 * b0, s1 = 1e-6 + a1 * a1 + 0.25 * b1 * b1,
                  s2 = 1e-6 + a2 * a2 + 0.25 * b2 * b2;
-    const double al0 = (1.0 / 16.0) / (s0 * s0), al1 = (5.0 / 8.0) / (s1 * s1), al2 = (5.0 / 16.0) / (s2 * s2);
+    double r0, r1, r2;
+    recip3(s0, s1, s2, r0, r1, r2);
+    const double al0 = (1.0 / 16.0) * (r0 * r0), al1 = (5.0 / 8.0) * (r1 * r1), al2 = (5.0 / 16.0) * (r2 * r2);
     const double u0 = 0.375 * q[0] - 1.25 * q[1] + 1.875 * q[2];
     const double u1 = -0.125 * q[1] + 0.75 * q[2] + 0.375 * q[3];
     const double u2 = 0.375 * q[2] + 0.75 * q[3] - 0.125 * q[4];
@@ -88,8 +110,8 @@ ADJ_HD void wcns5_adj(const double *q, double Qb, double *qb)
     const double g = Qb * iS;
     const double ub0 = g * al0, ub1 = g * al1, ub2 = g * al2;
     // d alpha_k / d beta_k = -2 alpha_k / s_k
-    const double bb0 = g * (u0 - Q) * (-2.0 * al0 / s0), bb1 = g * (u1 - Q) * (-2.0 * al1 / s1),
-                 bb2 = g * (u2 - Q) * (-2.0 * al2 / s2);
+    const double bb0 = g * (u0 - Q) * (-2.0 * al0 * r0), bb1 = g * (u1 - Q) * (-2.0 * al1 * r1),
+                 bb2 = g * (u2 - Q) * (-2.0 * al2 * r2);
     const double ab0 = 2.0 * a0 * bb0, bq0 = 0.5 * b0 * bb0;
     const double ab1 = 2.0 * a1 * bb1, bq1 = 0.5 * b1 * bb1;
     const double ab2 = 2.0 * a2 * bb2, bq2 = 0.5 * b2 * bb2;
@@ -190,7 +212,9 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
     const double VnL = vl[AX], VnR = vr[AX];
     const double s1 = sqrt(rl), s2 = sqrt(rr), iA = 1.0 / (s1 + s2), rhoA = s1 * s2;
     const double vA[2] = {(s1 * vl[0] + s2 * vr[0]) * iA, (s1 * vl[1] + s2 * vr[1]) * iA};
-    const double HL = 0.5 * kl + kGG1 * pl / rl, HR = 0.5 * kr + kGG1 * pr / rr;
+    // 1/rho of both states, for H here and for the reverse below
+    const double irl = 1.0 / rl, irr = 1.0 / rr;
+    const double HL = 0.5 * kl + kGG1 * pl * irl, HR = 0.5 * kr + kGG1 * pr * irr;
     const double HA = (s1 * HL + s2 * HR) * iA;
     const double q2 = 0.5 * (vA[0] * vA[0] + vA[1] * vA[1]);
     const double c2 = kGm1 * (HA - q2), c = sqrt(c2), ic2 = 1.0 / c2;
@@ -274,7 +298,7 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
     }
     VnAb += 0.05 * (VnA >= 0.0 ? epsb : -epsb);
     cb += 0.05 * epsb;
-    const double c2b = cb * 0.5 / c - ic2 * ic2 * ic2b;
+    const double c2b = cb * 0.5 * (c * ic2) - ic2 * ic2 * ic2b;  // 1/c = c / c^2
     HAb += kGm1 * c2b;
     q2b -= kGm1 * c2b;
     vAb[AX] += VnAb;
@@ -289,10 +313,11 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
     }
     s1b += s2 * rhoAb;
     s2b += s1 * rhoAb;
-    klb += 0.5 * HLb; plb += kGG1 / rl * HLb; rlb -= kGG1 * pl / (rl * rl) * HLb;
-    krb += 0.5 * HRb; prb += kGG1 / rr * HRb; rrb -= kGG1 * pr / (rr * rr) * HRb;
-    rlb += s1b * 0.5 / s1;
-    rrb += s2b * 0.5 / s2;
+    // 1/sqrt(rho) = sqrt(rho) / rho
+    klb += 0.5 * HLb; plb += kGG1 * irl * HLb; rlb -= kGG1 * pl * (irl * irl) * HLb;
+    krb += 0.5 * HRb; prb += kGG1 * irr * HRb; rrb -= kGG1 * pr * (irr * irr) * HRb;
+    rlb += s1b * 0.5 * (s1 * irl);
+    rrb += s2b * 0.5 * (s2 * irr);
     for (int i = 0; i < 2; i++) {
         vlb[i] += 2.0 * vl[i] * klb;
         vrb[i] += 2.0 * vr[i] * krb;
@@ -307,19 +332,21 @@ ADJ_HD void roe_vjp(const double *L, const double *R, const double *resb, double
 // L, columns of R) and what they are built from (eigenSystem.cpp:13-86)
 template <int AX>
 struct FaceEig {
-    double P2[4], P3[4], s1, s2, iA, HL, HR, u, v, ht, ek, h, c, ic, ih, Vn, L[4][4], R[4][4];
+    // i2, i3: 1/rho of cells 2 and 3
+    double P2[4], P3[4], i2, i3, s1, s2, iA, HL, HR, u, v, ht, ek, h, c, ic, ih, Vn, L[4][4], R[4][4];
     ADJ_HD explicit FaceEig(const double (&U)[6][4])
     {
         constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
-        c2p(U[2], P2);
-        c2p(U[3], P3);
+        i2 = c2p(U[2], P2);
+        i3 = c2p(U[3], P3);
         s1 = sqrt(P2[0]); s2 = sqrt(P3[0]); iA = 1.0 / (s1 + s2);
-        HL = 0.5 * (P2[1] * P2[1] + P2[2] * P2[2]) + kGG1 * P2[3] / P2[0];
-        HR = 0.5 * (P3[1] * P3[1] + P3[2] * P3[2]) + kGG1 * P3[3] / P3[0];
+        HL = 0.5 * (P2[1] * P2[1] + P2[2] * P2[2]) + kGG1 * P2[3] * i2;
+        HR = 0.5 * (P3[1] * P3[1] + P3[2] * P3[2]) + kGG1 * P3[3] * i3;
         u = (s1 * P2[1] + s2 * P3[1]) * iA; v = (s1 * P2[2] + s2 * P3[2]) * iA;
         ht = (s1 * HL + s2 * HR) * iA;
         ek = 0.5 * (u * u + v * v); h = ht - ek;
-        c = sqrt(kGm1 * h); ic = 1.0 / c; ih = 1.0 / h; Vn = nx * u + ny * v;
+        // c^2 = (gamma - 1) h, so 1/h = (gamma - 1) / c^2
+        c = sqrt(kGm1 * h); ic = 1.0 / c; ih = kGm1 * (ic * ic); Vn = nx * u + ny * v;
         L[0][0] = -ny * u + nx * v; L[0][1] = ny; L[0][2] = -nx; L[0][3] = 0.0;
         L[1][0] = h - ek; L[1][1] = u; L[1][2] = v; L[1][3] = -1.0;
         L[2][0] = 0.5 * (Vn * ic + ek * ih); L[2][1] = 0.5 * (-nx * ic - u * ih); L[2][2] = 0.5 * (-ny * ic - v * ih);
@@ -377,8 +404,7 @@ ADJ_HD void face_vjp_states(const double (&U)[6][4], const double *Fb, FaceState
         cl[i] = R[i][0] * QL[0] + R[i][1] * QL[1] + R[i][2] * QL[2] + R[i][3] * QL[3];
         cr[i] = R[i][0] * QR[0] + R[i][1] * QR[1] + R[i][2] * QR[2] + R[i][3] * QR[3];
     }
-    c2p(cl, fl);
-    c2p(cr, fr);
+    const double icl = c2p(cl, fl), icr = c2p(cr, fr);
     // positivity fallback (reconstructor5order.hpp:380-381), right state quirk included
     const bool fbl = fl[0] < 0 || fl[3] < 0, fbr = fr[0] < 0 || fr[3] < 0;
     if (fbl)
@@ -399,12 +425,12 @@ ADJ_HD void face_vjp_states(const double (&U)[6][4], const double *Fb, FaceState
     if (fbl) {
         for (int i = 0; i < 4; i++) P2b[i] += flb[i];
     } else {
-        c2p_adj(cl, fl, flb, clb);
+        c2p_adj(fl, icl, flb, clb);
     }
     if (fbr) {
         P3b[0] += frb[0]; P2b[1] += frb[1]; P2b[2] += frb[2]; P3b[3] += frb[3];
     } else {
-        c2p_adj(cr, fr, frb, crb);
+        c2p_adj(fr, icr, frb, crb);
     }
 }
 
@@ -501,12 +527,14 @@ ADJ_HD void face_vjp_chars(const double (&U)[6][4], const FaceStates &f, double 
     const double HLb = s1 * iA * htb, HRb = s2 * iA * htb;
     const double s1b = iA * ((P2[1] - u) * ub + (P2[2] - v) * vb + (HL - ht) * htb);
     const double s2b = iA * ((P3[1] - u) * ub + (P3[2] - v) * vb + (HR - ht) * htb);
-    P2b[1] += uLb + P2[1] * HLb; P2b[2] += vLb + P2[2] * HLb; P2b[3] += kGG1 / P2[0] * HLb;
-    P2b[0] += -kGG1 * P2[3] / (P2[0] * P2[0]) * HLb + s1b * 0.5 / s1;
-    P3b[1] += uRb + P3[1] * HRb; P3b[2] += vRb + P3[2] * HRb; P3b[3] += kGG1 / P3[0] * HRb;
-    P3b[0] += -kGG1 * P3[3] / (P3[0] * P3[0]) * HRb + s2b * 0.5 / s2;
-    c2p_adj(U[2], P2, P2b, Ub[2]);
-    c2p_adj(U[3], P3, P3b, Ub[3]);
+    // 1/rho and 1/sqrt(rho) = sqrt(rho)/rho of both cells from one reciprocal each
+    const double i2 = e.i2, i3 = e.i3;
+    P2b[1] += uLb + P2[1] * HLb; P2b[2] += vLb + P2[2] * HLb; P2b[3] += kGG1 * i2 * HLb;
+    P2b[0] += -kGG1 * P2[3] * (i2 * i2) * HLb + s1b * 0.5 * (s1 * i2);
+    P3b[1] += uRb + P3[1] * HRb; P3b[2] += vRb + P3[2] * HRb; P3b[3] += kGG1 * i3 * HRb;
+    P3b[0] += -kGG1 * P3[3] * (i3 * i3) * HRb + s2b * 0.5 * (s2 * i3);
+    c2p_adj(P2, i2, P2b, Ub[2]);
+    c2p_adj(P3, i3, P3b, Ub[3]);
 }
 
 // Forward face flux of stencil U[6][4] and Ub += (dF/dU)^T Fb; interpolation
@@ -526,7 +554,7 @@ ADJ_HD void node_vjp(const double *U, const double *Gb, double *cb)
 {
     constexpr double nx = (AX == 0) ? 1.0 : 0.0, ny = (AX == 1) ? 1.0 : 0.0;
     double p[4];
-    c2p(U, p);
+    const double ir = c2p(U, p);
     const double r = p[0], u = p[1], v = p[2], pp = p[3];
     const double Vn = nx * u + ny * v, q2 = u * u + v * v;
     double pb[4];
@@ -535,7 +563,7 @@ ADJ_HD void node_vjp(const double *U, const double *Gb, double *cb)
     pb[1] = r * Vn * Gb[1] + u * r * Vn * Gb[3] + nx * Vnb;
     pb[2] = r * Vn * Gb[2] + v * r * Vn * Gb[3] + ny * Vnb;
     pb[3] = nx * Gb[1] + ny * Gb[2] + kGG1 * Vn * Gb[3];
-    c2p_adj(U, p, pb, cb);
+    c2p_adj(p, ir, pb, cb);
 }
 
 
