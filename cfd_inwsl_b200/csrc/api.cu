@@ -386,6 +386,12 @@ struct cfd_handle {
     // adj_aux) and its reverse sweep (on the handle's stream)
     cudaGraphExec_t adj_recomp_graph[2] = {nullptr, nullptr};
     cudaGraphExec_t adj_back_graph[2] = {nullptr, nullptr};
+    // the record pass's last segment, run keeping its stage states in
+    // adj_stage (the first set of the reverse pass), so that the reverse pass
+    // starts without recomputing it; adj_last_valid until a reverse pass
+    // consumes them
+    cudaGraphExec_t adj_last_graph = nullptr;
+    bool adj_last_valid = false;
     std::vector<double *> adj_stage_b;   // the second set of stage states (overlap)
     cudaStream_t adj_aux = nullptr;      // recomputation stream of the reverse pass
     cudaEvent_t adj_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // recomputed[set], reversed[set]
@@ -644,6 +650,8 @@ void drop_graphs(cfd_handle *h)
         if (h->adj_back_graph[k]) cudaGraphExecDestroy(h->adj_back_graph[k]);
         h->adj_recomp_graph[k] = h->adj_back_graph[k] = nullptr;
     }
+    if (h->adj_last_graph) cudaGraphExecDestroy(h->adj_last_graph);
+    h->adj_last_graph = nullptr;
     h->adj_graph_K = 0;
 }
 
@@ -1932,13 +1940,15 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
     // cudaFree / cudaMalloc pair on the timed path of repeated gradients
     if ((rc = adjoint_states(h, h->adj_ckpt, nck))) return rc;
     const size_t state = sizeof(double) * h->ncell * h->nv;
+    const int K = ckpt_every;
+    h->adj_last_valid = false;
+    if ((rc = adjoint_states(h, h->adj_stage, 3 * (size_t)K + 1))) return rc;
     CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), h->stream));
     if (h->adj_graph_K != ckpt_every || h->adj_graph_dt != dt) {
         drop_graphs(h);
         h->adj_graph_K = ckpt_every;
         h->adj_graph_dt = dt;
     }
-    const int K = ckpt_every;
     // `cnt` steps from state slot `slot` (buffers by role)
     auto steps_from = [&](int slot, int cnt) -> int {
         for (int j = 0; j < cnt; j++) {
@@ -1949,10 +1959,33 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
         }
         return CFD_OK;
     };
+    // the last segment's steps with every stage state kept in adj_stage
+    // (the same launches as the reverse pass's recomputation of it)
+    auto keep_stages = [&](int cnt) -> int {
+        std::vector<double *> &st = h->adj_stage;
+        for (int j = 0; j < cnt; j++) {
+            double *S[3] = {st[3 * j], st[3 * j + 1], st[3 * j + 2]};
+            int r = adjoint_step(h, dt, S, st[3 * (j + 1)]);
+            if (r) return r;
+        }
+        return CFD_OK;
+    };
     for (int s0 = 0; s0 < nsteps; s0 += K) {
         const int cnt = std::min(K, nsteps - s0);
         CFD_CUDA(h, cudaMemcpyAsync(h->adj_ckpt[s0 / K], h->u[h->cur], state, cudaMemcpyDeviceToDevice, h->stream));
-        if (cnt == K) {  // a full segment: one graph per starting slot
+        if (s0 + cnt >= nsteps) {  // the last segment
+            CFD_CUDA(h, cudaMemcpyAsync(h->adj_stage[0], h->u[h->cur], state, cudaMemcpyDeviceToDevice, h->stream));
+            if (cnt == K) {
+                if (!h->adj_last_graph && (rc = capture_graph(h, [&] { return keep_stages(K); }, &h->adj_last_graph)))
+                    return rc;
+                CFD_CUDA(h, cudaGraphLaunch(h->adj_last_graph, h->stream));
+                h->launches += 3ULL * h->dim * K;
+            } else if ((rc = keep_stages(cnt))) {
+                return rc;
+            }
+            CFD_CUDA(h, cudaMemcpyAsync(h->u[(h->cur + cnt) % 3], h->adj_stage[3 * cnt], state,
+                                        cudaMemcpyDeviceToDevice, h->stream));
+        } else if (cnt == K) {  // a full segment: one graph per starting slot
             const int slot = h->cur;
             if (!h->adj_rec_graph[slot] &&
                 (rc = capture_graph(h, [&] { return steps_from(slot, K); }, &h->adj_rec_graph[slot])))
@@ -1971,7 +2004,9 @@ int cfd_adjoint_record(cfd_handle *h, double dt, int nsteps, int ckpt_every)
     unsigned err = 0;
     CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
     CFD_CUDA(h, cudaStreamSynchronize(h->stream));
-    return check_err(h, err);
+    rc = check_err(h, err);
+    h->adj_last_valid = (rc == CFD_OK);
+    return rc;
 }
 
 int cfd_run_fixed(cfd_handle *h, double dt, int nsteps, int steps_per_graph)
@@ -2031,6 +2066,10 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
     if ((rc = adjoint_supported(h)) || (rc = adjoint_buffers(h))) return rc;
     const int K = h->adj_every, N = h->adj_nsteps;
     const double dt = h->adj_dt;
+    // the record pass left the last segment's stage states in the first set
+    // (once: this pass overwrites that set)
+    const bool have_last = h->adj_last_valid;
+    h->adj_last_valid = false;
     if ((rc = adjoint_states(h, h->adj_stage, 3 * (size_t)K + 1))) return rc;
     const size_t state = sizeof(double) * h->ncell * h->nv;
     double *lam = h->adj_buf[0], *w = h->adj_buf[1], *w2 = h->adj_buf[2];
@@ -2124,7 +2163,8 @@ int cfd_adjoint_reverse(cfd_handle *h, const double *dJ_dUN_aos, double *dJ_dU0_
         return CFD_OK;
     };
     bool used[2] = {false, false};
-    if ((rc = launch_recompute(nseg - 1, 0))) return rc;
+    if (have_last) CFD_CUDA(h, cudaEventRecord(h->adj_ev[0], main_st));
+    else if ((rc = launch_recompute(nseg - 1, 0))) return rc;
     for (int seg = nseg - 1; seg >= 0; seg--) {
         const int set = (nseg - 1 - seg) & 1, other = set ^ 1;
         if (seg > 0) {

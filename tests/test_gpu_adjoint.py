@@ -188,6 +188,26 @@ def test_adjoint_matches_finite_differences(nsteps, ckpt, im):
     check_directions(g, U0, rng, diff, lambda U: objective(forward(f, U, dt, nsteps), probes))
 
 
+@pytest.mark.parametrize("nsteps,ckpt", [(12, 5), (10, 5), (4, 6)])
+def test_reverse_twice_after_one_record(nsteps, ckpt):
+    """The record pass keeps its last segment's stage states for the first
+    reverse pass, which then skips recomputing that segment; a second reverse
+    pass recomputes it from the checkpoint. Both give the same gradient, bit
+    for bit (full and partial last segments, one segment)."""
+    rng = np.random.default_rng(31 + nsteps)
+    nx, ny = 32, 28
+    s = solver(nx, ny)
+    U0 = smooth_periodic(nx, ny, rng, amp=0.1)
+    s.set_cons(U0)
+    dt = s.getTimeIntervalExplicit()
+    probes = rng.choice(nx * ny, 16, replace=False)
+    s.adjoint_record(dt, nsteps, ckpt)
+    sd = seed(s.cons, probes)
+    g1 = s.adjoint_reverse(sd)
+    g2 = s.adjoint_reverse(sd)
+    np.testing.assert_array_equal(g1, g2)
+
+
 @pytest.mark.parametrize("im", [2, 11])
 def test_adjoint_pinned_by_reference_forward(ref, im):
     """dJ/dU0 . d against central differences of the reference solver's own
