@@ -109,6 +109,12 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
 #define CFD_SWEEP_MINB128 4  // resident 128-thread CTAs per SM (2D/3D)
 #endif
 
+#if defined(CFD_FAST)
+constexpr bool kStrictFlavour = false;
+#else
+constexpr bool kStrictFlavour = true;
+#endif
+
 constexpr int pow2_ceil(int x)
 {
     int r = 1;
@@ -144,7 +150,10 @@ struct SweepShape {
     static constexpr bool THREE = ((FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5)) ||
                                   (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0) ||
                                   (CFD_FP64_2D_Y16 && PREC == 0 && NV == 4 && AX == 1);
-    static constexpr int MINB128 = THREE ? 3 : CFD_SWEEP_MINB128;
+    // The strict flavour's 3D z sweep (the stage-closing one) measured 7%
+    // faster at two CTAs per SM (255 registers) than at three.
+    static constexpr bool TWO = kStrictFlavour && PREC == 0 && NV == 5 && AX == 2;
+    static constexpr int MINB128 = TWO ? 2 : THREE ? 3 : CFD_SWEEP_MINB128;
     static constexpr int MINB = (NT <= 256) ? (NV >= 4 ? (NT == 128 ? MINB128 : CFD_SWEEP_MINB * (256 / NT))
                                                        : CFD_SWEEP_MINB)
                                             : 1;
