@@ -200,6 +200,21 @@ __global__ void division_check_kernel(long long n, unsigned long long seed, unsi
         const double got = cfd::div_rn(a, b, y), want = a / b;
         if (__double_as_longlong(got) != __double_as_longlong(want) || __double_as_longlong(y) != __double_as_longlong(1.0 / b))
             cnt++;
+        // the grouped form: a with two more dividends over the same b (a
+        // random one and, one time in four each, a signed zero or a dividend
+        // outside the corrected range), either sign of b
+        {
+            const unsigned long long k = splitmix64(st) % 8;
+            const double a2 = rand_double(st, -40, 40);
+            const double a3 = (k == 0) ? 0.0 : (k == 1) ? -0.0 : (k == 2) ? rand_double(st, 962, 1000)
+                                                                           : rand_double(st, -40, 40);
+            const double bs = (splitmix64(st) & 1) ? -b : b, ys = cfd::rcp_rn(bs);
+            const double A[3] = {a, a2, a3}, B[3] = {bs, bs, bs}, Y[3] = {ys, ys, ys};
+            double Q[3];
+            cfd::divs_rn<3>(A, B, Y, Q);
+            for (int j = 0; j < 3; j++)
+                if (__double_as_longlong(Q[j]) != __double_as_longlong(A[j] / bs)) cnt++;
+        }
     }
     if (cnt) atomicAdd(bad, cnt);
 }

@@ -46,10 +46,11 @@ constexpr double kRcpGm1 = 1.0 / kGm1;          // RN(1 / (gamma - 1))
 // one ulp away, so a first correction brings it within a small fraction of an
 // ulp and a second applies the theorem: five FP64 operations against about
 // thirteen FP64 issue slots for a division on B200 (measured). Dividends that
-// are zero, tiny (below 2^-960, where the residual could be subnormal), huge
-// or not finite take the IEEE division itself, so zeros keep their sign. The
-// denominators here are densities, sound speeds, enthalpies and spacings,
-// normal numbers far from the ends of the exponent range.
+// are tiny (below 2^-960, where the residual could be subnormal), huge or not
+// finite take the IEEE division itself; zeros keep their sign through the
+// sign of RN(a y). Quotients formed together share one test and one branch
+// (divs_rn). The denominators here are densities, sound speeds, enthalpies
+// and spacings, normal numbers far from the ends of the exponent range.
 // ---------------------------------------------------------------------------
 CFD_HD double rcp_rn(double b)
 {
@@ -67,19 +68,60 @@ CFD_HD double rcp_rn(double b)
 static __device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
 #endif
 
+#if defined(__CUDA_ARCH__)
+// Whether a's quotient may take the Markstein correction: 2^-960 <= |a| <
+// 2^960 (biased exponent 63..1982) or a = +-0, tested on the bits with integer
+// operations (no FP64 compares on the FP64 pipe).
+__device__ __forceinline__ bool mk_ok(double a)
+{
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
+    const unsigned e = (unsigned)(bits >> 52) & 0x7ffu;
+    return (e - 63u <= 1919u) | ((bits << 1) == 0ull);
+}
+
+// Markstein's quotient of a by b from y = RN(1/b). The sign is taken from
+// q0 = RN(a y), which carries sign(a) sign(b) also for a = +-0, where the
+// corrections can turn -0 into +0.
+__device__ __forceinline__ double mk_div(double a, double b, double y)
+{
+    const double q0 = a * y;
+    double r = fma(-b, q0, a);
+    const double q = fma(r, y, q0);
+    r = fma(-b, q, a);
+    return copysign(fma(r, y, q), q0);
+}
+#endif
+
 CFD_HD double div_rn(double a, double b, double y)
 {
 #if defined(__CUDA_ARCH__)
-    const double aa = fabs(a);
-    if (!(aa >= 0x1p-960 && aa <= 0x1p960)) return div_ieee(a, b);
-    double q = a * y;
-    double r = fma(-b, q, a);
-    q = fma(r, y, q);
-    r = fma(-b, q, a);
-    return fma(r, y, q);
+    const double q = mk_div(a, b, y);
+    return mk_ok(a) ? q : div_ieee(a, b);
 #else
     (void)y;
     return a / b;
+#endif
+}
+
+// q[i] = RN(a[i] / b[i]), y[i] = RN(1/b[i]), for N quotients formed together:
+// one branch to the IEEE division for the group instead of one per quotient.
+template <int N>
+CFD_HD void divs_rn(const double *a, const double *b, const double *y, double *q)
+{
+#if defined(__CUDA_ARCH__)
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        q[i] = mk_div(a[i], b[i], y[i]);
+        ok = ok & mk_ok(a[i]);
+    }
+    if (!ok) {
+#pragma unroll
+        for (int i = 0; i < N; i++) q[i] = div_ieee(a[i], b[i]);
+    }
+#else
+    (void)y;
+    for (int i = 0; i < N; i++) q[i] = a[i] / b[i];
 #endif
 }
 
@@ -582,8 +624,10 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         double E = rE * ir;
 #else
         const double ir = rcp_rn(r);
-        double u = div_rn(ru, r, ir);
-        double E = div_rn(rE, r, ir);
+        const double a[2] = {ru, rE}, bb[2] = {r, r}, yy[2] = {ir, ir};
+        double qq[2];
+        divs_rn<2>(a, bb, yy, qq);
+        double u = qq[0], E = qq[1];
 #endif
         double e = -u * u / 2 + E;
         double RT = (gamma - 1) * e;
@@ -595,7 +639,10 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         double u = ru * ir, v = rv * ir, E = rE * ir;
 #else
         const double ir = rcp_rn(r);
-        double u = div_rn(ru, r, ir), v = div_rn(rv, r, ir), E = div_rn(rE, r, ir);
+        const double a[3] = {ru, rv, rE}, bb[3] = {r, r, r}, yy[3] = {ir, ir, ir};
+        double qq[3];
+        divs_rn<3>(a, bb, yy, qq);
+        double u = qq[0], v = qq[1], E = qq[2];
 #endif
         double q2 = (u * u + v * v) / 2;
         double e = -q2 + E;
@@ -608,7 +655,10 @@ CFD_HD void cons_to_prim(const double *c, double *p)
         double u = ru * ir, v = rv * ir, w = rw * ir, E = rE * ir;
 #else
         const double ir = rcp_rn(r);
-        double u = div_rn(ru, r, ir), v = div_rn(rv, r, ir), w = div_rn(rw, r, ir), E = div_rn(rE, r, ir);
+        const double a[4] = {ru, rv, rw, rE}, bb[4] = {r, r, r, r}, yy[4] = {ir, ir, ir, ir};
+        double qq[4];
+        divs_rn<4>(a, bb, yy, qq);
+        double u = qq[0], v = qq[1], w = qq[2], E = qq[3];
 #endif
         double q2 = (u * u + v * v + w * w) / 2;
         double e = -q2 + E;
@@ -851,8 +901,11 @@ CFD_HD void char_cons_to_prim(const double *cs, double *p)
         double rekt = (rut * rut + rvt * rvt) * (0.5 * irt);
 #else
         const double irt = rcp_rn(rt);
-        double ut = div_rn(rut, rt, irt), vt = div_rn(rvt, rt, irt);
-        double rekt = div_rn(rut * rut + rvt * rvt, rt, irt) / 2;
+        const double a[3] = {rut, rvt, rut * rut + rvt * rvt}, bb[3] = {rt, rt, rt}, yy[3] = {irt, irt, irt};
+        double qq[3];
+        divs_rn<3>(a, bb, yy, qq);
+        double ut = qq[0], vt = qq[1];
+        double rekt = qq[2] / 2;
 #endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = (gamma - 1) * (ret - rekt);
     } else {
@@ -863,8 +916,12 @@ CFD_HD void char_cons_to_prim(const double *cs, double *p)
         double rekt = (rut * rut + rvt * rvt + rwt * rwt) * (0.5 * irt);
 #else
         const double irt = rcp_rn(rt);
-        double ut = div_rn(rut, rt, irt), vt = div_rn(rvt, rt, irt), wt = div_rn(rwt, rt, irt);
-        double rekt = div_rn(rut * rut + rvt * rvt + rwt * rwt, rt, irt) / 2;
+        const double a[4] = {rut, rvt, rwt, rut * rut + rvt * rvt + rwt * rwt}, bb[4] = {rt, rt, rt, rt},
+                     yy[4] = {irt, irt, irt, irt};
+        double qq[4];
+        divs_rn<4>(a, bb, yy, qq);
+        double ut = qq[0], vt = qq[1], wt = qq[2];
+        double rekt = qq[3] / 2;
 #endif
         p[0] = rt; p[1] = ut; p[2] = vt; p[3] = wt; p[4] = (gamma - 1) * (ret - rekt);
     }
@@ -1068,11 +1125,18 @@ struct EigenBase {
         c = sqrt((gamma - 1) * h);
         ic = rcp_rn(c);
         ih = rcp_rn(h);
-        Vc = div_rn(Vn, c, ic);
-        ekh = div_rn(ek, h, ih);
-        uh = div_rn(u, h, ih);
-        vh = div_rn(v, h, ih);
-        wh = (D == 3) ? div_rn(w, h, ih) : 0.0;
+        if constexpr (D == 2) {
+            const double a[4] = {Vn, ek, u, v}, bb[4] = {c, h, h, h}, yy[4] = {ic, ih, ih, ih};
+            double qq[4];
+            divs_rn<4>(a, bb, yy, qq);
+            Vc = qq[0]; ekh = qq[1]; uh = qq[2]; vh = qq[3];
+            wh = 0.0;
+        } else {
+            const double a[5] = {Vn, ek, u, v, w}, bb[5] = {c, h, h, h, h}, yy[5] = {ic, ih, ih, ih, ih};
+            double qq[5];
+            divs_rn<5>(a, bb, yy, qq);
+            Vc = qq[0]; ekh = qq[1]; uh = qq[2]; vh = qq[3]; wh = qq[4];
+        }
 #endif
     }
 
@@ -1330,13 +1394,18 @@ CFD_HD void hllc_md(const double *L, const double *R, double *res)
     double cl = sqrt(prl * gamma), cr = sqrt(prr * gamma);
 #else
     const double prl = pl / rl, prr = pr / rr;
-    // x / (gamma - 1) by its correctly rounded reciprocal (div_rn)
-    if constexpr (D == 2) {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + div_rn(prl * kGamma, kGm1, kRcpGm1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + div_rn(prr * kGamma, kGm1, kRcpGm1);
-    } else {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + div_rn(prl * kGamma, kGm1, kRcpGm1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + div_rn(prr * kGamma, kGm1, kRcpGm1);
+    // x / (gamma - 1) by its correctly rounded reciprocal (divs_rn)
+    {
+        const double a[2] = {prl * kGamma, prr * kGamma}, bb[2] = {kGm1, kGm1}, yy[2] = {kRcpGm1, kRcpGm1};
+        double qq[2];
+        divs_rn<2>(a, bb, yy, qq);
+        if constexpr (D == 2) {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + qq[0];
+            HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + qq[1];
+        } else {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + qq[0];
+            HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + qq[1];
+        }
     }
     double VnL = vl[AX], VnR = vr[AX];
     double cl = sqrt(prl * gamma), cr = sqrt(prr * gamma);
@@ -1490,13 +1559,18 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     double rl = L[0], rr = R[0], pl = L[E], pr = R[E];
     const double *vl = L + 1, *vr = R + 1;
     double HL, HR;
-    // x / (gamma - 1) by its correctly rounded reciprocal (div_rn)
-    if constexpr (D == 2) {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + div_rn(pl / rl * kGamma, kGm1, kRcpGm1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + div_rn(pr / rr * kGamma, kGm1, kRcpGm1);
-    } else {
-        HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + div_rn(pl / rl * kGamma, kGm1, kRcpGm1);
-        HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + div_rn(pr / rr * kGamma, kGm1, kRcpGm1);
+    // x / (gamma - 1) by its correctly rounded reciprocal (divs_rn)
+    {
+        const double a[2] = {pl / rl * kGamma, pr / rr * kGamma}, bb[2] = {kGm1, kGm1}, yy[2] = {kRcpGm1, kRcpGm1};
+        double qq[2];
+        divs_rn<2>(a, bb, yy, qq);
+        if constexpr (D == 2) {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1]) / 2 + qq[0];
+            HR = (vr[0] * vr[0] + vr[1] * vr[1]) / 2 + qq[1];
+        } else {
+            HL = (vl[0] * vl[0] + vl[1] * vl[1] + vl[2] * vl[2]) / 2 + qq[0];
+            HR = (vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]) / 2 + qq[1];
+        }
     }
     double VnL = vl[AX], VnR = vr[AX];
     double FcL[NV], FcR[NV];
@@ -1534,17 +1608,23 @@ CFD_HD void roe_md(const double *L, const double *R, double *res)
     // the three quotients by c^2 and 2 c^2 from one correctly rounded
     // reciprocal: (2 c) c = 2 RN(c c) exactly, so x / (2 c c) = RN(x / (c c)) / 2
     const double cc2 = cAvg * cAvg, icc2 = rcp_rn(cc2);
-    double c1 = div_rn(deltaP - rhoAvg * cAvg * deltaVn, cc2, icc2) / 2;
+    double qc[3];
+    {
+        const double a[3] = {deltaP - rhoAvg * cAvg * deltaVn, deltaP + rhoAvg * cAvg * deltaVn, deltaP},
+                     bb[3] = {cc2, cc2, cc2}, yy[3] = {icc2, icc2, icc2};
+        divs_rn<3>(a, bb, yy, qc);
+    }
+    double c1 = qc[0] / 2;
     Fd[0] = lambda[0] * (c1 * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] = lambda[0] * (c1 * (vAvg[i] - cAvg * n[i]));
     Fd[E] = lambda[0] * (c1 * (HAvg - cAvg * VnAvg));
 
-    double cc = div_rn(deltaP + rhoAvg * cAvg * deltaVn, cc2, icc2) / 2;
+    double cc = qc[1] / 2;
     Fd[0] += lambda[2] * (cc * 1);
     for (int i = 0; i < D; i++) Fd[1 + i] += lambda[2] * (cc * (vAvg[i] + cAvg * n[i]));
     Fd[E] += lambda[2] * (cc * (HAvg + cAvg * VnAvg));
 
-    double c2 = deltaRho - div_rn(deltaP, cc2, icc2);
+    double c2 = deltaRho - qc[2];
     Fd[0] += lambda[1] * (c2 * 1.0 + rhoAvg * 0.0);
     // tangential components carry rhoAvg * dv_i, the normal one 0
     // (fluxSchemes.hpp:526-528 for axis normals).
@@ -1601,6 +1681,13 @@ CFD_HD void node_flux(const double *p, double *f)
 
 // MidNodeAndNodeDif6 (differ.cpp:54-103): one cell's contribution,
 // (w1 (Fn[i+1]-Fn[i-1]) + w0 (Fh[i+1/2]-Fh[i-1/2]) + w2 (Fh[i+3/2]-Fh[i-3/2])) / h.
+// The numerator of mnd6 (the difference before the division by h).
+CFD_HD double mnd6_num(double fnm1, double fnp1, double fhm3, double fhm1, double fhp1, double fhp3)
+{
+    const double w0 = 3.0 / 2.0, w1 = -3.0 / 10.0, w2 = 1.0 / 30.0;
+    return w1 * (fnp1 - fnm1) + w0 * (fhp1 - fhm1) + w2 * (fhp3 - fhm3);
+}
+
 CFD_HD double mnd6(double fnm1, double fnp1, double fhm3, double fhm1, double fhp1, double fhp3, double h,
                    double inv_h)
 {

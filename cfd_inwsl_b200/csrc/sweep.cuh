@@ -447,12 +447,34 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
 #pragma unroll
             for (int m = 0; m <= FC; m++) fs[m] = fring(i - (FC - 1) / 2 + m - s_begin + FO);
             const long long cell = base + (long long)i * sAX;
+            // MND6 differences of the NV variables (strict: the NV quotients by
+            // h formed together, one branch for the group)
+            double dd[NV];
+            if constexpr (DIFF == 0) {
+#if defined(CFD_FAST)
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const double *fv = sf + (v * W + tl) * LSF;
+                    dd[v] = mnd6(fnm[v], fnp[v], fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]], p.h, inv_h);
+                }
+#else
+                double num[NV], hh[NV], ihh[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const double *fv = sf + (v * W + tl) * LSF;
+                    num[v] = mnd6_num(fnm[v], fnp[v], fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]]);
+                    hh[v] = p.h;
+                    ihh[v] = inv_h;
+                }
+                divs_rn<NV>(num, hh, ihh, dd);
+#endif
+            }
             double uo[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 const double *fv = sf + (v * W + tl) * LSF;
                 double d;
-                if constexpr (DIFF == 0) d = mnd6(fnm[v], fnp[v], fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]], p.h, inv_h);
+                if constexpr (DIFF == 0) d = dd[v];
                 else d = trad6(fv[fs[0]], fv[fs[1]], fv[fs[2]], fv[fs[3]], fv[fs[4]], fv[fs[5]], p.h, inv_h);
                 const long long gi = v * p.ncell + cell;
                 const double *sv = stg + v * NT + tid;

@@ -192,8 +192,9 @@ int cfd_fp64_peak_probe(long long iters, void *stream, double *flops);
 /* Self-check of the strict flavour's correctly rounded division by a shared
  * reciprocal (Markstein's correction) against the device's IEEE division on n
  * seeded operand pairs (random, next to rounding midpoints, physical ranges,
- * signed zeros, tiny and huge dividends); *mismatches counts pairs whose
- * quotient or reciprocal bits differ. No counterpart in the reference: it
+ * signed zeros, tiny and huge dividends), each also in the grouped form
+ * (three dividends over one divisor of either sign); *mismatches counts
+ * quotients or reciprocals whose bits differ. No counterpart in the reference: it
  * backs the strict flavour's bit-for-bit parity. */
 int cfd_check_division(long long n, unsigned long long seed, unsigned long long *mismatches);
 
