@@ -71,6 +71,8 @@ _PROTOS = {
     "cfd_rk3_step": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "cfd_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                           C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
+    "cfd_step_host": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double)]),
     "cfd_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong),
                                    C.POINTER(C.c_void_p)]),
     "cfd_set_state_device": (C.c_int, [C.c_void_p, C.c_void_p]),

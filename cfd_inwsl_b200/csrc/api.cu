@@ -36,19 +36,22 @@ constexpr int kGhost = 4;
 
 // ------------------------------------------------------------------ kernels
 
+// The transposes and the wave-speed reduction work on the cells [c0, c1).
 template <int NV>
-__global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__restrict__ soa, long long ncell)
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__restrict__ soa, long long ncell,
+                                  long long c0, long long c1)
 {
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+    for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1; c += (long long)gridDim.x * blockDim.x) {
 #pragma unroll
         for (int v = 0; v < NV; v++) soa[v * ncell + c] = aos[c * NV + v];
     }
 }
 
 template <int NV>
-__global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__restrict__ aos, long long ncell, int to_prim)
+__global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__restrict__ aos, long long ncell, int to_prim,
+                                  long long c0, long long c1)
 {
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+    for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1; c += (long long)gridDim.x * blockDim.x) {
         double x[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) x[v] = soa[v * ncell + c];
@@ -67,11 +70,12 @@ __global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__rest
 // as getTimeIntervalExplicit's OpenMP max loops (blockSolver.cpp:327-338).
 template <int NV>
 __global__ void __launch_bounds__(256) wave_speed_kernel(const double *__restrict__ u, long long ncell, double h0,
-                                                          double h1, double h2, unsigned long long *red)
+                                                          double h1, double h2, unsigned long long *red, long long c0,
+                                                          long long c1)
 {
     double lam[3] = {0.0, 0.0, 0.0};
     const double hd[3] = {h0, h1, h2};
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+    for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1; c += (long long)gridDim.x * blockDim.x) {
         double x[NV], p[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) x[v] = u[v * ncell + c];
@@ -351,6 +355,9 @@ InterMap map_inter_method(int m, int dim)
 
 } // namespace
 
+// chunks of the overlapped host step (cfd_step_host), each direction
+constexpr int kHostChunks = 8;
+
 struct cfd_handle {
     cfd_config cfg;
     int dim = 0, nv = 0;
@@ -410,6 +417,9 @@ struct cfd_handle {
     std::vector<double *> adj_stage_b;   // the second set of stage states (overlap)
     cudaStream_t adj_aux = nullptr;      // recomputation stream of the reverse pass
     cudaEvent_t adj_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // recomputed[set], reversed[set]
+    // cfd_step_host: the copy stream and one event per chunk and direction
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t host_ev[2][kHostChunks] = {};
     int adj_graph_K = 0;
     double adj_graph_dt = 0.0;
     // slab decomposition: halo rows of the last direction's low / high side
@@ -539,23 +549,27 @@ int grid_for(long long n)
     return (int)g;
 }
 
-int launch_aos_to_soa(cfd_handle *h, const double *aos, double *soa)
+int launch_aos_to_soa(cfd_handle *h, const double *aos, double *soa, long long c0 = 0, long long c1 = -1)
 {
-    int g = grid_for(h->ncell);
-    if (h->nv == 3) aos_to_soa_kernel<3><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
-    else if (h->nv == 4) aos_to_soa_kernel<4><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
-    else aos_to_soa_kernel<5><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell);
+    if (c1 < 0) c1 = h->ncell;
+    if (c1 <= c0) return CFD_OK;
+    int g = grid_for(c1 - c0);
+    if (h->nv == 3) aos_to_soa_kernel<3><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell, c0, c1);
+    else if (h->nv == 4) aos_to_soa_kernel<4><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell, c0, c1);
+    else aos_to_soa_kernel<5><<<g, 256, 0, h->stream>>>(aos, soa, h->ncell, c0, c1);
     CFD_CUDA(h, cudaGetLastError());
     h->launches++;
     return CFD_OK;
 }
 
-int launch_soa_to_aos(cfd_handle *h, const double *soa, double *aos, int to_prim)
+int launch_soa_to_aos(cfd_handle *h, const double *soa, double *aos, int to_prim, long long c0 = 0, long long c1 = -1)
 {
-    int g = grid_for(h->ncell);
-    if (h->nv == 3) soa_to_aos_kernel<3><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
-    else if (h->nv == 4) soa_to_aos_kernel<4><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
-    else soa_to_aos_kernel<5><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim);
+    if (c1 < 0) c1 = h->ncell;
+    if (c1 <= c0) return CFD_OK;
+    int g = grid_for(c1 - c0);
+    if (h->nv == 3) soa_to_aos_kernel<3><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim, c0, c1);
+    else if (h->nv == 4) soa_to_aos_kernel<4><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim, c0, c1);
+    else soa_to_aos_kernel<5><<<g, 256, 0, h->stream>>>(soa, aos, h->ncell, to_prim, c0, c1);
     CFD_CUDA(h, cudaGetLastError());
     h->launches++;
     return CFD_OK;
@@ -617,27 +631,37 @@ int rhs_all(cfd_handle *h, const double *u, double t)
 }
 
 // One RK stage: RHS of uin, then uout = combination (blockSolver.cpp:51-86).
-int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, double *uout, double A, double Bdt,
-             double C, double t, bool reduce, const cfd::StepCtl *ctl = nullptr)
+// The sweep along d of one RK stage: a partial RHS for the leading
+// directions, the stage combination in the last one.
+SweepParams stage_params(cfd_handle *h, int d, int stage, const double *uin, const double *u0, double *uout, double A,
+                         double Bdt, double C, double t, bool reduce, const cfd::StepCtl *ctl)
 {
-    for (int d = 0; d < h->dim; d++) {
-        SweepParams p = base_params(h, d);
-        p.u = uin;
-        p.u0 = u0;
-        p.rhs = h->rhs;
-        p.u_out = uout;
-        bool last = (d == h->dim - 1);
-        p.mode = last ? cfd::MODE_RK : cfd::MODE_WRITE;
-        p.first = (d == 0);
-        p.rk_stage = stage;
-        p.rkA = A;
-        p.rkBdt = Bdt;
-        p.rkC = C;
-        p.want_reduce = (reduce && last) ? 1 : 0;
-        p.t = t;
-        p.ctl = ctl;
-        p.gravity = (h->cfg.source_type == 1 && last) ? 1 : 0;
-        int rc = sweep(h, d, p);
+    SweepParams p = base_params(h, d);
+    p.u = uin;
+    p.u0 = u0;
+    p.rhs = h->rhs;
+    p.u_out = uout;
+    bool last = (d == h->dim - 1);
+    p.mode = last ? cfd::MODE_RK : cfd::MODE_WRITE;
+    p.first = (d == 0);
+    p.rk_stage = stage;
+    p.rkA = A;
+    p.rkBdt = Bdt;
+    p.rkC = C;
+    p.want_reduce = (reduce && last) ? 1 : 0;
+    p.t = t;
+    p.ctl = ctl;
+    p.gravity = (h->cfg.source_type == 1 && last) ? 1 : 0;
+    return p;
+}
+
+// the sweeps of one RK stage along directions [d0, d1) (d1 < 0: all)
+int rk_stage(cfd_handle *h, int stage, const double *uin, const double *u0, double *uout, double A, double Bdt,
+             double C, double t, bool reduce, const cfd::StepCtl *ctl = nullptr, int d0 = 0, int d1 = -1)
+{
+    if (d1 < 0) d1 = h->dim;
+    for (int d = d0; d < d1; d++) {
+        int rc = sweep(h, d, stage_params(h, d, stage, uin, u0, uout, A, Bdt, C, t, reduce, ctl));
         if (rc) return rc;
     }
     return CFD_OK;
@@ -698,16 +722,27 @@ int check_err(cfd_handle *h, unsigned err)
     return CFD_OK;
 }
 
+// wave-speed maxima of the current state's cells [c0, c1) folded into red
+// (the caller clears red before the first range)
+int launch_wave_speed_range(cfd_handle *h, long long c0, long long c1)
+{
+    if (c1 <= c0) return CFD_OK;
+    int g = grid_for(c1 - c0);
+    const double *u = h->u[h->cur];
+    const double *hh = h->cfg.h;
+    if (h->nv == 3) wave_speed_kernel<3><<<g, 256, 0, h->stream>>>(u, h->ncell, hh[0], hh[1], hh[2], h->red, c0, c1);
+    else if (h->nv == 4) wave_speed_kernel<4><<<g, 256, 0, h->stream>>>(u, h->ncell, hh[0], hh[1], hh[2], h->red, c0, c1);
+    else wave_speed_kernel<5><<<g, 256, 0, h->stream>>>(u, h->ncell, hh[0], hh[1], hh[2], h->red, c0, c1);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    return CFD_OK;
+}
+
 int launch_wave_speed(cfd_handle *h)
 {
     CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), h->stream));
-    int g = grid_for(h->ncell);
-    const double *u = h->u[h->cur];
-    if (h->nv == 3) wave_speed_kernel<3><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-    else if (h->nv == 4) wave_speed_kernel<4><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-    else wave_speed_kernel<5><<<g, 256, 0, h->stream>>>(u, h->ncell, h->cfg.h[0], h->cfg.h[1], h->cfg.h[2], h->red);
-    CFD_CUDA(h, cudaGetLastError());
-    h->launches++;
+    int rc = launch_wave_speed_range(h, 0, h->ncell);
+    if (rc) return rc;
     h->ws_valid = true;
     return CFD_OK;
 }
@@ -909,6 +944,13 @@ void cfd_destroy(cfd_handle *h)
     }
     for (cudaEvent_t ev : h->adj_ev)
         if (ev) cudaEventDestroy(ev);
+    if (h->copy_st) {
+        cudaStreamSynchronize(h->copy_st);
+        cudaStreamDestroy(h->copy_st);
+    }
+    for (auto &row : h->host_ev)
+        for (cudaEvent_t ev : row)
+            if (ev) cudaEventDestroy(ev);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
@@ -1093,6 +1135,108 @@ int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_s
     if (k > 0 && linf) CFD_CUDA(h, cudaMemcpy(linf, h->d_linf, sizeof(double) * k, cudaMemcpyDeviceToHost));
     unsigned err;
     CFD_CUDA(h, cudaMemcpy(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost));
+    return check_err(h, err);
+}
+
+int cfd_step_host(cfd_handle *h, double cfl, double output_dt, const double *in_aos, double *out_aos, double *t,
+                  double *dt)
+{
+    if (!h || !in_aos || !out_aos || !t || !(output_dt > 0.0)) return CFD_ERR_CONFIG;
+    const int L = h->dim - 1;
+    const long long nL = h->cfg.n[L];
+    const long long plane = h->ncell / nL;  // cells per index of the last dimension
+    const long long seg = h->seg_len[L];
+    const long long nseg = (nL + seg - 1) / seg;
+    int rc;
+    if (h->dim < 2 || nL < 64 || nseg < 2) {
+        // too small to overlap: the three calls in turn
+        if ((rc = cfd_upload_cons(h, in_aos))) return rc;
+        int ns = 0;
+        double dts[1] = {0.0};
+        if ((rc = cfd_run(h, cfl, 1, output_dt, 1, t, &ns, dts, nullptr))) return rc;
+        if (dt) *dt = ns ? dts[0] : 0.0;
+        return cfd_download_cons(h, out_aos);
+    }
+    if ((rc = sync_bc(h)) || (rc = ensure_run_buffers(h, 1))) return rc;
+    if (!h->copy_st) CFD_CUDA(h, cudaStreamCreateWithFlags(&h->copy_st, cudaStreamNonBlocking));
+    for (auto &row : h->host_ev)
+        for (cudaEvent_t &ev : row)
+            if (!ev) CFD_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaStream_t st = h->stream, cs = h->copy_st;
+    const size_t cell_bytes = sizeof(double) * h->nv;
+    // step control as cfd_run(h, cfl, 1, output_dt, 1) sets it; the first
+    // sweep of stage 1 runs before step_begin_kernel, so its stage time (the
+    // current t) is set here as well
+    cfd::StepCtl *c = h->ctl_host;
+    std::memset(c, 0, sizeof(*c));
+    c->t = *t;
+    c->outputDt = output_dt;
+    c->cfl = cfl;
+    c->endStep = 1;
+    c->maxSteps = 1;
+    c->tst[1] = *t;
+    CFD_CUDA(h, cudaMemcpyAsync(h->ctl, c, sizeof(*c), cudaMemcpyHostToDevice, st));
+    CFD_CUDA(h, cudaMemsetAsync(h->err, 0, sizeof(unsigned), st));
+    CFD_CUDA(h, cudaMemsetAsync(h->red, 0, 4 * sizeof(unsigned long long), st));
+    // the copies start after the work queued so far on the handle's stream
+    CFD_CUDA(h, cudaEventRecord(h->host_ev[1][0], st));
+    CFD_CUDA(h, cudaStreamWaitEvent(cs, h->host_ev[1][0], 0));
+    const int cur = h->cur;
+    double *U0 = h->u[cur], *U1 = h->u[(cur + 1) % 3], *U2 = h->u[(cur + 2) % 3];
+    // Upload in chunks of lines of the last dimension (multiples of 32, which
+    // every first-direction tile height divides): each chunk is transposed,
+    // its wave speeds folded into the reduction and its lines of the first
+    // sweep of stage 1 (which needs no dt) computed while the next one copies.
+    const long long lines_up = ((nL + kHostChunks - 1) / kHostChunks + 31) / 32 * 32;
+    int k = 0;
+    for (long long r0 = 0; r0 < nL; r0 += lines_up, k++) {
+        const long long r1 = std::min(nL, r0 + lines_up), c0 = r0 * plane, c1 = r1 * plane;
+        CFD_CUDA(h, cudaMemcpyAsync(h->stage + c0 * h->nv, in_aos + c0 * h->nv, (c1 - c0) * cell_bytes,
+                                    cudaMemcpyHostToDevice, cs));
+        CFD_CUDA(h, cudaEventRecord(h->host_ev[0][k], cs));
+        CFD_CUDA(h, cudaStreamWaitEvent(st, h->host_ev[0][k], 0));
+        if ((rc = launch_aos_to_soa(h, h->stage, U0, c0, c1)) || (rc = launch_wave_speed_range(h, c0, c1))) return rc;
+        SweepParams p = stage_params(h, 0, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
+        p.part_lo = (int)r0;
+        p.part_hi = (int)r1;
+        if ((rc = sweep(h, 0, p))) return rc;
+    }
+    step_begin_kernel<<<1, 1, 0, st>>>(h->ctl, h->red, h->dim, h->d_dts);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    if ((rc = rk_stage(h, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl, 1)) ||
+        (rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl)) ||
+        (rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl, 0, L)))
+        return rc;
+    // The last sweep of stage 3 in chunks of whole segments along the last
+    // dimension: each chunk is transposed and copied out while the next one
+    // is computed.
+    const long long segs_dn = (nseg + kHostChunks - 1) / kHostChunks;
+    k = 0;
+    for (long long s0 = 0; s0 < nseg; s0 += segs_dn, k++) {
+        const long long r0 = s0 * seg, r1 = std::min(nL, (s0 + segs_dn) * seg), c0 = r0 * plane, c1 = r1 * plane;
+        SweepParams p = stage_params(h, L, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl);
+        p.part_lo = (int)r0;
+        p.part_hi = (int)r1;
+        p.seg_outer = 1;
+        if ((rc = sweep(h, L, p)) || (rc = launch_soa_to_aos(h, U1, h->stage, 0, c0, c1))) return rc;
+        CFD_CUDA(h, cudaEventRecord(h->host_ev[1][k], st));
+        CFD_CUDA(h, cudaStreamWaitEvent(cs, h->host_ev[1][k], 0));
+        CFD_CUDA(h, cudaMemcpyAsync(out_aos + c0 * h->nv, h->stage + c0 * h->nv, (c1 - c0) * cell_bytes,
+                                    cudaMemcpyDeviceToHost, cs));
+    }
+    step_end_kernel<<<1, 1, 0, st>>>(h->ctl, h->red, h->d_linf);
+    CFD_CUDA(h, cudaGetLastError());
+    h->launches++;
+    CFD_CUDA(h, cudaMemcpyAsync(c, h->ctl, sizeof(*c), cudaMemcpyDeviceToHost, st));
+    unsigned err = 0;
+    CFD_CUDA(h, cudaMemcpyAsync(&err, h->err, sizeof(err), cudaMemcpyDeviceToHost, st));
+    CFD_CUDA(h, cudaStreamSynchronize(st));
+    CFD_CUDA(h, cudaStreamSynchronize(cs));
+    h->cur = (cur + c->k) % 3;
+    *t = c->t;
+    if (dt) *dt = c->dt;
+    h->ws_valid = true;  // stage 3 left the next step's wave speeds in red[1..3]
     return check_err(h, err);
 }
 

@@ -216,8 +216,15 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
     const int nseg = (nd + p.seg_len - 1) / p.seg_len;
     const int nblk0 = (nt0 + W - 1) / W;
     int bid = block_id;
-    const int seg = bid % nseg;
-    bid /= nseg;
+    int seg;
+    if (p.seg_outer) {  // segments outermost (partial sweeps along the last dimension)
+        const int per = nblk0 * p.n[T1];
+        seg = bid / per;
+        bid -= seg * per;
+    } else {
+        seg = bid % nseg;
+        bid /= nseg;
+    }
     const int a0 = (bid % nblk0) * W;
     const int bb = bid / nblk0;
     const int s_begin = seg * p.seg_len;
@@ -533,7 +540,7 @@ template <int NV, int AX, int FAM, int FLUX, int S, int W, int PREC, int DIFF>
 __global__ void __launch_bounds__(S *W, (SweepShape<NV, AX, FAM, FLUX, S, W, PREC, DIFF>::MINB))
     sweep_kernel(const __grid_constant__ SweepParams p)
 {
-    sweep_tile<NV, AX, FAM, FLUX, S, W, PREC, DIFF>(p, blockIdx.x);
+    sweep_tile<NV, AX, FAM, FLUX, S, W, PREC, DIFF>(p, (int)(p.tile0 + blockIdx.x));
 }
 
 // Number of CTA tiles one case's sweep along AX needs.
@@ -600,10 +607,33 @@ static cudaError_t launch_sweep_shape_p(const SweepParams &p, cudaStream_t st)
     constexpr int T0 = (AX == 0) ? 1 : 0;
     constexpr int T1 = (AX == 2) ? 1 : 2;
     long long nseg = (p.n[AX] + p.seg_len - 1) / p.seg_len;
-    long long nblk = (long long)((p.n[T0] + W - 1) / W) * p.n[T1] * nseg;
-    if (nblk <= 0) return cudaSuccess;
+    const long long nblk0 = (p.n[T0] + W - 1) / W;
+    long long nblk = nblk0 * p.n[T1] * nseg;
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC, DIFF><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(p);
+    SweepParams q = p;
+    q.tile0 = 0;
+    if (p.part_lo < p.part_hi) {
+        // the tiles covering [part_lo, part_hi) of the last dimension L
+        const int L = (p.n[2] > 1) ? 2 : 1;
+        if (AX == L) {  // whole segments, segments outermost
+            if (!p.seg_outer) return cudaErrorInvalidValue;
+            const long long s0 = p.part_lo / p.seg_len, s1 = (p.part_hi + p.seg_len - 1) / p.seg_len;
+            q.tile0 = s0 * nblk0 * p.n[T1];
+            nblk = (s1 - s0) * nblk0 * p.n[T1];
+        } else if (T0 == L) {  // lines of L in blocks of W (2D)
+            if (p.part_lo % W) return cudaErrorInvalidValue;
+            const long long b0 = p.part_lo / W, b1 = (p.part_hi + W - 1) / W;
+            q.tile0 = b0 * nseg;
+            nblk = (b1 - b0) * nseg;
+        } else {  // planes of L (3D)
+            q.tile0 = (long long)p.part_lo * nblk0 * nseg;
+            nblk = (long long)(p.part_hi - p.part_lo) * nblk0 * nseg;
+        }
+    } else if (p.seg_outer) {
+        return cudaErrorInvalidValue;
+    }
+    if (nblk <= 0) return cudaSuccess;
+    sweep_kernel<NV, AX, FAM, FLUX, S, W, PREC, DIFF><<<(unsigned)nblk, SH::NT, SH::SMEM_BYTES, st>>>(q);
     return cudaGetLastError();
 }
 

@@ -124,6 +124,14 @@ struct SweepParams {
     long long halo_nl;                // lines per halo row
     int diff;                         // DIFF_TRAD6: ExplicitDif6 with 5 ghosts; else MND6 with 4
     int posl;                         // 1: the 1D positivity limiter on 2D/3D face states (cfd_config.positivity)
+    // Partial sweeps (cfd_step_host): part_lo < part_hi restricts the launch
+    // to the lines and segments covering indices [part_lo, part_hi) of the
+    // grid's last dimension (for a sweep along it, whole segments, with
+    // seg_outer = 1 so that they are a contiguous tile range). tile0: first
+    // tile of the launch (set by the launcher).
+    int part_lo, part_hi;
+    int seg_outer;
+    long long tile0;
 };
 
 // One batched sweep launch: the parameter blocks of every case (device array)

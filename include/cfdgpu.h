@@ -158,6 +158,22 @@ int cfd_rk3_step(cfd_handle *h, double dt, double t, double *rho_linf);
 int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_steps, double *t, int *nsteps,
             double *dts, double *linf);
 
+/* One CFL step from a host state to a host state, both in the reference's
+ * AoS layout (BlockSolver::RK3_SSP with getTimeIntervalExplicit's dt, as one
+ * step of stepsLoopCFL, blockSolver.cpp:43-87 and :170-235, for host code
+ * that keeps its Data on the host between steps): equal bit for bit to
+ * cfd_upload_cons(in_aos) + cfd_run(h, cfl, 1, output_dt, 1, t, ...) +
+ * cfd_download_cons(out_aos). The copies overlap the step: the upload runs in
+ * chunks along the last dimension, each chunk transposed, its wave speeds
+ * reduced and its lines of stage 1's first sweep computed while the next one
+ * copies; the last sweep of stage 3 runs in chunks of whole segments, each
+ * downloaded while the next is computed. in_aos and out_aos may be the same
+ * buffer; pinned host memory lets the copies run asynchronously. *t is
+ * advanced; *dt (may be NULL) receives the step size. 1D grids and grids of
+ * fewer than 64 cells along the last dimension take the three calls in turn. */
+int cfd_step_host(cfd_handle *h, double cfl, double output_dt, const double *in_aos, double *out_aos, double *t,
+                  double *dt);
+
 /* Device pointers and CUDA stream of the handle, for callers that keep the
  * state resident (e.g. a framework tensor sharing the buffer). state receives
  * the current conserved state in the device layout: planar SoA
