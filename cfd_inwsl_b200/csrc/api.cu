@@ -419,6 +419,9 @@ struct cfd_handle {
     cudaEvent_t adj_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // recomputed[set], reversed[set]
     // cfd_step_host: the copy stream and one event per chunk and direction
     cudaStream_t copy_st = nullptr;
+    // a line end of direction d was wired by cfd_set_line_bc (its ghost cells
+    // may come from any cell of the grid)
+    bool line_bc_set[3] = {false, false, false};
     cudaEvent_t host_ev[2][kHostChunks] = {};
     int adj_graph_K = 0;
     double adj_graph_dt = 0.0;
@@ -967,6 +970,7 @@ int cfd_set_line_bc(cfd_handle *h, int idim, int i, int j, int side, int bnd_typ
     transverse_axes(d, t0, t1);
     if (i < 0 || i >= h->cfg.n[t0] || j < 0 || j >= h->cfg.n[t1]) return fail(h, CFD_ERR_CONFIG, "line index out of range");
     if (bnd_type == CFD_BND_HALO) return fail(h, CFD_ERR_CONFIG, "halo ends are wired by cfd_enable_halo");
+    h->line_bc_set[d] = true;
     // BndType values (macro.hpp:33-34) and the true wrap; anything else would
     // leave the line end's ghosts undefined
     if (!((bnd_type >= CFD_BND_TYPENULL && bnd_type <= CFD_BND_SYMMETRYZ) || bnd_type == CFD_BND_PERIODIC_WRAP))
@@ -1185,34 +1189,72 @@ int cfd_step_host(cfd_handle *h, double cfl, double output_dt, const double *in_
     double *U0 = h->u[cur], *U1 = h->u[(cur + 1) % 3], *U2 = h->u[(cur + 2) % 3];
     // Upload in chunks of lines of the last dimension (multiples of 32, which
     // every first-direction tile height divides): each chunk is transposed,
-    // its wave speeds folded into the reduction and its lines of the first
-    // sweep of stage 1 (which needs no dt) computed while the next one copies.
+    // its wave speeds folded into the reduction and its lines of stage 1's
+    // leading sweeps computed while the next one copies. Stage 1's last sweep
+    // (which needs no dt until its combination) runs as a partial RHS in
+    // whole segments as soon as their cells and ghost sources are in: the
+    // last chunk is uploaded first, so the periodic wrap of the first
+    // segments is there. With line ends wired by cfd_set_line_bc along the
+    // last direction (ghosts from anywhere) it waits for the whole upload.
+    // dt then gives the stage-1 combination (rk_combine), the flavour's own
+    // rounding of the epilogue it replaces.
     const long long lines_up = ((nL + kHostChunks - 1) / kHostChunks + 31) / 32 * 32;
-    int k = 0;
-    for (long long r0 = 0; r0 < nL; r0 += lines_up, k++) {
-        const long long r1 = std::min(nL, r0 + lines_up), c0 = r0 * plane, c1 = r1 * plane;
+    const int nup = (int)((nL + lines_up - 1) / lines_up);
+    const long long tail0 = (long long)(nup - 1) * lines_up;  // first row of the last chunk
+    const bool early_last = !h->line_bc_set[L];
+    const long long halo = 5;  // ghost cells each side of a segment (4 with MND6, 5 with TRAD6)
+    long long avail = 0, next_seg = 0;
+    auto last_sweep_write = [&](long long s0, long long s1) -> int {
+        if (s1 <= s0) return CFD_OK;
+        SweepParams p = stage_params(h, L, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
+        p.mode = cfd::MODE_WRITE;  // the RHS only; rk_combine applies the stage
+        p.part_lo = (int)(s0 * seg);
+        p.part_hi = (int)std::min(nL, s1 * seg);
+        p.seg_outer = 1;
+        return sweep(h, L, p);
+    };
+    for (int i = 0; i < nup; i++) {
+        const int k = (i == 0) ? nup - 1 : i - 1;  // the last chunk first
+        const long long r0 = k * lines_up, r1 = std::min(nL, r0 + lines_up), c0 = r0 * plane, c1 = r1 * plane;
         CFD_CUDA(h, cudaMemcpyAsync(h->stage + c0 * h->nv, in_aos + c0 * h->nv, (c1 - c0) * cell_bytes,
                                     cudaMemcpyHostToDevice, cs));
-        CFD_CUDA(h, cudaEventRecord(h->host_ev[0][k], cs));
-        CFD_CUDA(h, cudaStreamWaitEvent(st, h->host_ev[0][k], 0));
+        CFD_CUDA(h, cudaEventRecord(h->host_ev[0][i], cs));
+        CFD_CUDA(h, cudaStreamWaitEvent(st, h->host_ev[0][i], 0));
         if ((rc = launch_aos_to_soa(h, h->stage, U0, c0, c1)) || (rc = launch_wave_speed_range(h, c0, c1))) return rc;
-        SweepParams p = stage_params(h, 0, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
-        p.part_lo = (int)r0;
-        p.part_hi = (int)r1;
-        if ((rc = sweep(h, 0, p))) return rc;
+        for (int d = 0; d < L; d++) {
+            SweepParams p = stage_params(h, d, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
+            p.part_lo = (int)r0;
+            p.part_hi = (int)r1;
+            if ((rc = sweep(h, d, p))) return rc;
+        }
+        if (k != nup - 1) avail = r1;  // rows [0, avail) and [tail0, nL) are in
+        if (!early_last) continue;
+        // segment s needs rows [s seg - halo, (s + 1) seg + halo), wrapped; the
+        // wrap of the first ones lies in the last chunk if that holds halo rows
+        const long long s_end = (avail >= tail0) ? nseg : (nL - tail0 < halo) ? 0 : std::max(0LL, (avail - halo) / seg);
+        if (s_end > next_seg) {
+            if ((rc = last_sweep_write(next_seg, s_end))) return rc;
+            next_seg = s_end;
+        }
     }
+    if ((rc = last_sweep_write(next_seg, nseg))) return rc;
     step_begin_kernel<<<1, 1, 0, st>>>(h->ctl, h->red, h->dim, h->d_dts);
     CFD_CUDA(h, cudaGetLastError());
     h->launches++;
-    if ((rc = rk_stage(h, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl, 1)) ||
-        (rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl)) ||
+    {
+        SweepParams p = stage_params(h, L, 1, U0, U0, U1, 1.0, 0.0, 0.0, 0.0, false, h->ctl);
+        cudaError_t e = cfd::launch_rk_combine_any(h->strict, h->nv, p, st);
+        if (e != cudaSuccess) return cuda_fail(h, e, "stage combination launch");
+        h->launches++;
+    }
+    if ((rc = rk_stage(h, 2, U1, U0, U2, 0.75, 0.0, 0.25, 0.0, false, h->ctl)) ||
         (rc = rk_stage(h, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl, 0, L)))
         return rc;
     // The last sweep of stage 3 in chunks of whole segments along the last
     // dimension: each chunk is transposed and copied out while the next one
     // is computed.
     const long long segs_dn = (nseg + kHostChunks - 1) / kHostChunks;
-    k = 0;
+    int k = 0;
     for (long long s0 = 0; s0 < nseg; s0 += segs_dn, k++) {
         const long long r0 = s0 * seg, r1 = std::min(nL, (s0 + segs_dn) * seg), c0 = r0 * plane, c1 = r1 * plane;
         SweepParams p = stage_params(h, L, 3, U2, U0, U1, 1.0 / 3.0, 0.0, 2.0 / 3.0, 0.0, true, h->ctl);

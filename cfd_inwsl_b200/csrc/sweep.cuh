@@ -790,3 +790,48 @@ cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStre
 
 } // namespace CFD_NS
 } // namespace cfd
+
+namespace cfd {
+namespace CFD_NS {
+
+// The RK stage combination of the last sweep's epilogue, applied by itself to
+// a complete RHS in p.rhs (the last sweep having run with MODE_WRITE):
+// U_out = (A U0 - Bdt R) + C U_k (stage 1: U0 - dt R) with the epilogue's
+// non-finite check. Compiled in the flavour's own unit, so it rounds the
+// expression as the fused epilogue does. No reductions: it serves stage 1.
+template <int NV>
+__global__ void __launch_bounds__(256) rk_combine_kernel(const __grid_constant__ SweepParams p)
+{
+    if (p.ctl && p.ctl->done) return;
+    const double rkBdt = p.ctl ? p.ctl->bdt[p.rk_stage] : p.rkBdt;
+    unsigned err = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < p.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        bool fin = true;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const long long gi = v * p.ncell + c;
+            const double r = p.rhs[gi];
+            double o;
+            if (p.rk_stage == 1) o = p.u0[gi] - rkBdt * r;
+            else o = p.rkA * p.u0[gi] - rkBdt * r + p.rkC * p.u[gi];
+            p.u_out[gi] = o;
+            fin = fin && isfinite(o);
+        }
+        if (!fin) err |= ERR_NONFINITE;
+    }
+    if (err) atomicOr(p.err, err);
+}
+
+template <int NV>
+cudaError_t launch_rk_combine(const SweepParams &p, cudaStream_t st)
+{
+    long long g = (p.ncell + 255) / 256;
+    if (g > 148LL * 16) g = 148LL * 16;
+    if (g < 1) g = 1;
+    rk_combine_kernel<NV><<<(unsigned)g, 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+} // namespace CFD_NS
+} // namespace cfd

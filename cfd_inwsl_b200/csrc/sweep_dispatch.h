@@ -9,12 +9,16 @@ template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st);
 template <int NV, int FAM>
 cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStream_t st);
+template <int NV>
+cudaError_t launch_rk_combine(const SweepParams &p, cudaStream_t st);
 }
 namespace fast {
 template <int NV, int FAM>
 cudaError_t launch_sweep(int ax, int flux, const SweepParams &p, cudaStream_t st);
 template <int NV, int FAM>
 cudaError_t launch_sweep_batched(int ax, int flux, const BatchSweep &b, cudaStream_t st);
+template <int NV>
+cudaError_t launch_rk_combine(const SweepParams &p, cudaStream_t st);
 }
 
 #define CFD_FOR_EACH_FAMILY(X) X(0) X(1) X(2) X(3) X(4) X(5)
@@ -33,6 +37,15 @@ inline cudaError_t launch_sweep_any(bool strict_flavour, int nv, int fam, int ax
     CFD_FOR_EACH_FAMILY(CFD_CASES_NV)
 #undef CFD_CASES_NV
 #undef CFD_CASE
+    return cudaErrorInvalidValue;
+}
+
+// The stage combination by itself (rk_combine_kernel), in the flavour's rounding.
+inline cudaError_t launch_rk_combine_any(bool strict_flavour, int nv, const SweepParams &p, cudaStream_t st)
+{
+    if (nv == 3) return strict_flavour ? strict::launch_rk_combine<3>(p, st) : fast::launch_rk_combine<3>(p, st);
+    if (nv == 4) return strict_flavour ? strict::launch_rk_combine<4>(p, st) : fast::launch_rk_combine<4>(p, st);
+    if (nv == 5) return strict_flavour ? strict::launch_rk_combine<5>(p, st) : fast::launch_rk_combine<5>(p, st);
     return cudaErrorInvalidValue;
 }
 

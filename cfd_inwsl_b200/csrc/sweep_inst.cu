@@ -6,5 +6,8 @@ namespace cfd {
 namespace CFD_NS {
 template cudaError_t launch_sweep<CFD_NV, CFD_FAM>(int ax, int flux, const SweepParams &p, cudaStream_t st);
 template cudaError_t launch_sweep_batched<CFD_NV, CFD_FAM>(int ax, int flux, const BatchSweep &b, cudaStream_t st);
+#if CFD_FAM == 0
+template cudaError_t launch_rk_combine<CFD_NV>(const SweepParams &p, cudaStream_t st);
+#endif
 } // namespace CFD_NS
 } // namespace cfd

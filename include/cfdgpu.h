@@ -165,9 +165,10 @@ int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_s
  * cfd_upload_cons(in_aos) + cfd_run(h, cfl, 1, output_dt, 1, t, ...) +
  * cfd_download_cons(out_aos). The copies overlap the step: the upload runs in
  * chunks along the last dimension, each chunk transposed, its wave speeds
- * reduced and its lines of stage 1's first sweep computed while the next one
- * copies; the last sweep of stage 3 runs in chunks of whole segments, each
- * downloaded while the next is computed. in_aos and out_aos may be the same
+ * reduced and its lines of stage 1's leading sweeps computed while the next
+ * one copies, stage 1's last sweep as a partial RHS as soon as its segments'
+ * cells are in; the last sweep of stage 3 runs in chunks of whole segments,
+ * each downloaded while the next is computed. in_aos and out_aos may be the same
  * buffer; pinned host memory lets the copies run asynchronously. *t is
  * advanced; *dt (may be NULL) receives the step size. 1D grids and grids of
  * fewer than 64 cells along the last dimension take the three calls in turn. */

@@ -3,8 +3,9 @@ overlapped with the sweeps) against cfd_upload_cons + cfd_run (one step) +
 cfd_download_cons. Both run the same kernels on the same data, the first in
 chunks along the last dimension, so states, dt and t agree bit for bit: grids
 whose chunks end ragged, 2D and 3D, strict, fast and mixed, the gravity source
-(nCase 3), the time-dependent DoubleMachUp boundary (nCase 4), an in-place
-buffer, and a grid small enough to take the unchunked path."""
+(nCase 3), the time-dependent DoubleMachUp boundary (nCase 4), outlets, a
+last chunk shorter than a segment's ghost cells, an in-place buffer, and a
+grid small enough to take the unchunked path."""
 import ctypes as C
 
 import numpy as np
@@ -75,6 +76,19 @@ def test_teno_roe_2d(flavour):
                               strict=flavour == "strict", precision=1 if flavour == "mixed" else 0,
                               seg_len=(0, 24, 0))
     compare(make, c, 0.4)
+
+
+def test_short_last_chunk_and_outlets():
+    """194 rows: the last upload chunk holds 2 rows, fewer than a segment's
+    ghost cells, so stage 1's last sweep waits for the whole upload (periodic
+    wrap); then the same grid with outlets from the configuration, whose
+    ghosts come from the line's own cells."""
+    nx, ny = 100, 194
+    c = smooth_2d(nx, ny, np.random.default_rng(11))
+    for periodic in (True, False):
+        make = lambda: gpu_solver(2, [nx, ny], im=11, fm=1, periodic=periodic, cfl=0.4, strict=True,
+                                  seg_len=(0, 16, 0))
+        compare(make, c, 0.4)
 
 
 def test_default_segments_2d_in_place():
