@@ -431,7 +431,7 @@ def adjoint_cost(device, stream, n=256, nsteps=400, ckpt=20, seed=0):
             "J": J, "grad_l2": float(np.linalg.norm(out["g"]))}
 
 
-def batch_throughput(device, stream, ncases=256, steps=20, seed=0, full_run=True):
+def batch_throughput(device, stream, ncases=256, steps=20, seed=0, full_run=True, subset=None):
     """Batched configuration: 256 independent 2D Riemann problems on [0,1]^2,
     N = round(2^U(7,10)) cells per side (seeded), quadrant states rho ~
     U[0.1,2], p ~ U[0.05,2], u, v ~ U[-1,1], WCNS5 + HLLC, CFL 0.5, per-case dt,
@@ -439,10 +439,14 @@ def batch_throughput(device, stream, ncases=256, steps=20, seed=0, full_run=True
     sweep (fast flavour; the strict flavour equals the reference case by case).
     Timed with CUDA events on the batch's stream: `steps` steps of every case
     with the default tiling and after cfd_batch_autotune, then (full_run) the
-    whole configuration, every case to t = 0.25."""
+    whole configuration, every case to t = 0.25. subset: the indices of the
+    cases this rank runs (replicas over GPUs), default all."""
     import torch
     from cfd_inwsl_b200 import _lib, cases, zone
     sizes, prims = cases.riemann_batch(ncases, seed)
+    if subset is not None:
+        sizes = [sizes[i] for i in subset]
+        prims = [prims[i] for i in subset]
     infos = []
     for n in sizes:
         info = zone.Info()
@@ -481,7 +485,7 @@ def batch_throughput(device, stream, ncases=256, steps=20, seed=0, full_run=True
     ms, cell_steps, _ = timed_run(steps)
     out = {"config": f"{ncases} cases, N = round(2^U(7,10)) (seeded, {min(sizes)}..{max(sizes)}), "
                      "WCNS5 + HLLC, CFL 0.5, transmissive, per-case dt, fast flavour",
-           "cells": int(sum(n * n for n in sizes)), "steps_per_case": steps, "ms": ms,
+           "cells": int(sum(n * n for n in sizes)), "steps_per_case": steps, "ms": ms, "cell_steps": cell_steps,
            "value": cell_steps / (ms / 1e3), "unit": "cell-steps/s",
            "autotuned_tiling": tiling, "default_tiling_value": cs0 / (ms0 / 1e3)}
     if full_run:
@@ -711,6 +715,23 @@ def run_ours(args, rank, world, local_rank):
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_throughput(local_rank, stream, full_run=args.batch_full)
+    elif not args.no_batch:
+        # replicas: the 256 cases split over the ranks by cost (N^3), no
+        # exchange; time = the slowest rank's, value = all ranks' cell-steps
+        from cfd_inwsl_b200 import cases as _cases
+        from cfd_inwsl_b200.replicas import case_cost, partition_by_cost
+        sizes_all, _ = _cases.riemann_batch(256, 0)
+        shares = partition_by_cost([case_cost(n) for n in sizes_all], world)
+        mine = batch_throughput(local_rank, stream, full_run=False, subset=shares[rank])
+        ms_b = max_over_ranks(mine["ms"])
+        import torch.distributed as dist
+        tot = torch.tensor([mine["cell_steps"]], dtype=torch.float64, device=dev)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        batch = {"config": mine["config"].replace(f"{len(shares[rank])} cases", "256 cases"),
+                 "parallelism": f"replicas: cases split over {world} ranks by cost N^3 (LPT), no exchange",
+                 "cases_per_rank": [len(sh) for sh in shares], "steps_per_case": mine["steps_per_case"],
+                 "ms": ms_b, "value": float(tot.item()) / (ms_b / 1e3), "unit": "cell-steps/s",
+                 "scaling": "strong"}
     tgv = None
     if not args.no_tgv and world == 1 and dim == 2:
         tgv = tgv_block(local_rank, stream, peak_tflops=peak_tflops)

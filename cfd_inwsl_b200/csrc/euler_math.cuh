@@ -74,9 +74,9 @@ static __device__ __noinline__ double div_ieee(double a, double b) { return a / 
 // operations (no FP64 compares on the FP64 pipe).
 __device__ __forceinline__ bool mk_ok(double a)
 {
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
-    const unsigned e = (unsigned)(bits >> 52) & 0x7ffu;
-    return (e - 63u <= 1919u) | ((bits << 1) == 0ull);
+    // t = |a|'s high word: biased exponent in bits 20..30
+    const unsigned t = (unsigned)__double2hiint(a) & 0x7fffffffu, lo = (unsigned)__double2loint(a);
+    return (t - (63u << 20) < (1920u << 20)) | ((t | lo) == 0u);
 }
 
 // Markstein's quotient of a by b from y = RN(1/b). The sign is taken from
