@@ -103,6 +103,22 @@ CFD_HD double div_rn(double a, double b, double y)
 #endif
 }
 
+#if defined(__CUDACC__)
+template <int N>
+struct DivN {
+    double v[N];
+};
+// A group's IEEE divisions, out of line (one call site per group)
+template <int N>
+static __device__ __noinline__ DivN<N> divs_ieee(DivN<N> a, DivN<N> b)
+{
+    DivN<N> q;
+#pragma unroll
+    for (int i = 0; i < N; i++) q.v[i] = a.v[i] / b.v[i];
+    return q;
+}
+#endif
+
 // q[i] = RN(a[i] / b[i]), y[i] = RN(1/b[i]), for N quotients formed together:
 // one branch to the IEEE division for the group instead of one per quotient.
 template <int N>
@@ -116,8 +132,15 @@ CFD_HD void divs_rn(const double *a, const double *b, const double *y, double *q
         ok = ok & mk_ok(a[i]);
     }
     if (!ok) {
+        DivN<N> A, B;
 #pragma unroll
-        for (int i = 0; i < N; i++) q[i] = div_ieee(a[i], b[i]);
+        for (int i = 0; i < N; i++) {
+            A.v[i] = a[i];
+            B.v[i] = b[i];
+        }
+        const DivN<N> Q = divs_ieee<N>(A, B);
+#pragma unroll
+        for (int i = 0; i < N; i++) q[i] = Q.v[i];
     }
 #else
     (void)y;

@@ -102,6 +102,22 @@ __device__ __forceinline__ void ghost_prim(const SweepParams &p, const BcLine &b
     }
 }
 
+template <int NV>
+struct PrimVals {
+    double v[NV];
+};
+
+// The same out of line, returned by value: boundary ghosts are a few cells
+// per line end, and one copy of this code instead of one per cell-loader call
+// site keeps the sweep's instruction footprint small.
+template <int NV, int NG>
+__device__ __noinline__ PrimVals<NV> ghost_prim_ool(const SweepParams &p, const BcLine &bl, int k, double tstage)
+{
+    PrimVals<NV> r;
+    ghost_prim<NV, NG>(p, bl, k, tstage, r.v);
+    return r;
+}
+
 #ifndef CFD_SWEEP_MINB
 #define CFD_SWEEP_MINB 2
 #endif
@@ -279,10 +295,14 @@ __device__ __forceinline__ void sweep_tile(const SweepParams &p, int block_id)
             have_cs = (PREC == 1);
         } else if (P < 0) {
             int k = -P - 1;
-            ghost_prim<NV, HG>(p, p.bc_lo[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
+            const PrimVals<NV> g = ghost_prim_ool<NV, HG>(p, p.bc_lo[lid], k > HG - 1 ? HG - 1 : k, tstage);
+#pragma unroll
+            for (int v = 0; v < NV; v++) pr[v] = g.v[v];
         } else {
             int k = P - nd;
-            ghost_prim<NV, HG>(p, p.bc_hi[lid], k > HG - 1 ? HG - 1 : k, tstage, pr);
+            const PrimVals<NV> g = ghost_prim_ool<NV, HG>(p, p.bc_hi[lid], k > HG - 1 ? HG - 1 : k, tstage);
+#pragma unroll
+            for (int v = 0; v < NV; v++) pr[v] = g.v[v];
         }
         if (!have_cs) prim_to_cons<NV>(pr, cs);  // as the reference's primToChar re-derives them
         int slot = ring(P - s_begin + HG);
