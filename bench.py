@@ -13,9 +13,10 @@ timed beside it).
 
   value   device-resident stepping (state in HBM, dt on the device), timed
           with CUDA events on the stream the kernels run on, max over ranks;
-  e2e     the same through the C ABI with host buffers: every step uploads the
-          state from pinned host memory, steps, and downloads the state and
-          the log values (dt, rhoLinf);
+  e2e     the same through the C ABI with host buffers: every step is one
+          cfd_step_host call that uploads the state from pinned host memory,
+          takes one CFL step and downloads the new state, the copies
+          overlapped with the step's sweeps (slabs: upload, step, download);
   roofline  the dominant kernel (the stage-closing sweep, which carries the
           stage's compulsory traffic: read U^k and U^0, write U^(k+1)), with
           its FP64 throughput against a DFMA peak measured in the same run;
@@ -28,7 +29,8 @@ periodic grid split into slabs along the last direction, each rank an n^dim
 tile (weak scaling): before every RK stage neighbouring slabs exchange their
 four boundary rows by NCCL point-to-point, and every step takes dt from a MAX
 all-reduce of the ranks' wave speeds; value = all ranks' cell-steps / max rank
-time.
+time. The batch block then runs the 256 independent cases as replicas, split
+over the ranks by cost (no exchange).
 """
 from __future__ import annotations
 
