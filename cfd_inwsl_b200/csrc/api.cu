@@ -1146,6 +1146,8 @@ int cfd_step_host(cfd_handle *h, double cfl, double output_dt, const double *in_
                   double *dt)
 {
     if (!h || !in_aos || !out_aos || !t || !(output_dt > 0.0)) return CFD_ERR_CONFIG;
+    if (h->halo[0] || h->halo[1])
+        return fail(h, CFD_ERR_UNSUPPORTED, "cfd_step_host: slab halos need an exchange before every stage");
     const int L = h->dim - 1;
     const long long nL = h->cfg.n[L];
     const long long plane = h->ncell / nL;  // cells per index of the last dimension

@@ -171,7 +171,9 @@ int cfd_run(cfd_handle *h, double cfl, int end_step, double output_dt, int max_s
  * each downloaded while the next is computed. in_aos and out_aos may be the same
  * buffer; pinned host memory lets the copies run asynchronously. *t is
  * advanced; *dt (may be NULL) receives the step size. 1D grids and grids of
- * fewer than 64 cells along the last dimension take the three calls in turn. */
+ * fewer than 64 cells along the last dimension take the three calls in turn.
+ * A handle with slab halos (cfd_enable_halo) is refused (CFD_ERR_UNSUPPORTED):
+ * its stages need halo exchanges in between. */
 int cfd_step_host(cfd_handle *h, double cfl, double output_dt, const double *in_aos, double *out_aos, double *t,
                   double *dt);
 

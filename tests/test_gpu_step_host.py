@@ -135,3 +135,20 @@ def test_double_mach_time_dependent_boundary(ref):
     make = lambda: zone.BlockSolver(make_info(2, n, zone_, im=2, fm=0, strict=True, ncase=4, cfl=0.5,
                                               seg_len=(0, 8, 0)))
     compare(make, c, 0.5, steps=3, t0=0.01)
+
+
+def test_slab_handle_is_refused():
+    """A handle with slab halos needs an exchange between stages, which the
+    host step does not do: refused before any work, the state untouched."""
+    rng = np.random.default_rng(2)
+    c = smooth_2d(64, 96, rng)
+    s = gpu_solver(2, [64, 96], im=2, fm=1, periodic=True, strict=True)
+    s.set_cons(c)
+    buf, cnt = C.c_void_p(), C.c_longlong(0)
+    _lib.check(s.lib.cfd_enable_halo(s.h, 0, C.byref(buf), C.byref(cnt)), s.h)
+    out = np.zeros_like(c)
+    tt, dt = C.c_double(0.0), C.c_double(0.0)
+    rc = s.lib.cfd_step_host(s.h, 0.5, 1e300, _lib.ptr(c), _lib.ptr(out), C.byref(tt), C.byref(dt))
+    assert rc == -6 and tt.value == 0.0
+    assert not out.any()
+    s.close()
