@@ -161,10 +161,12 @@ struct SweepShape {
     // Resident CTAs per SM the launch bounds ask for: 512 threads per SM in
     // 2D/3D (two CTAs of 256 threads or four of 128), 128 registers a thread;
     // or three 128-thread CTAs (168 registers, fewer spills), which measured
-    // faster for the FP64 y sweep (2D), the FP64 y and z sweeps (3D), the
-    // FP64 TENO-Z x sweep and the 3D mixed TENO-Z sweeps.
+    // faster for the FP64 y sweep (2D), every FP64 3D sweep (the x sweep
+    // spilled 880 / 576 bytes per thread at 128 registers in the strict /
+    // fast flavour: 3.35 -> 3.23 and 1.90 -> 1.78 ms per 256^3 launch at
+    // three CTAs), the FP64 TENO-Z x sweep and the 3D mixed TENO-Z sweeps.
     static constexpr bool THREE = ((FAM == FAM_TENOZ) && (PREC == 0 ? AX == 0 : NV == 5)) ||
-                                  (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5 && AX != 0) ||
+                                  (CFD_FP64_3D_YZ16 && PREC == 0 && NV == 5) ||
                                   (CFD_FP64_2D_Y16 && PREC == 0 && NV == 4 && AX == 1);
     // The strict flavour's 3D z sweep (the stage-closing one) measured 7%
     // faster at two CTAs per SM (255 registers) than at three.
