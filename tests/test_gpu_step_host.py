@@ -152,3 +152,19 @@ def test_slab_handle_is_refused():
     assert rc == -6 and tt.value == 0.0
     assert not out.any()
     s.close()
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_trad6_five_ghosts(periodic):
+    """The TRAD6 difference reads five cells beyond a segment's ends; the
+    host step's early stage-1 sweep waits for them (periodic wrap and
+    outlets)."""
+    nx, ny = 96, 160
+    c = smooth_2d(nx, ny, np.random.default_rng(21))
+
+    def make():
+        info = make_info(2, [nx, ny], im=2, fm=0, strict=True, cfl=0.5, seg_len=(0, 16, 0))
+        info.diffMethod = zone.DiffMethod.TRAD6
+        return zone.BlockSolver(info, periodic=periodic)
+
+    compare(make, c, 0.5)
